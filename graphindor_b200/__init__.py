@@ -1,0 +1,279 @@
+"""graphindor_b200: a B200-native graph pattern-counting engine.
+
+Python mirror of the reference's host interface (Pattern, Schedule_IEP,
+Graph and the pattern_matching / clique / motif entry points) over the C ABI
+in include/gi.h.  Every count runs in the CUDA library; there is no CPU
+fallback: if the library or a GPU is missing, the calls raise.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+from typing import Optional, Sequence
+
+import numpy as np
+
+from . import _native as N
+from ._native import GIError, check, lib
+
+__all__ = ["Pattern", "Schedule_IEP", "Graph", "pattern_matching", "clique_count", "motif_counting",
+           "motif_patterns", "GIError", "lib", "write_g", "read_g"]
+
+
+class Pattern:
+    """n-vertex pattern from the reference's n*n '0'/'1' string (reference
+    src/pattern.cpp:22-31: any '1' at (i, j) adds the undirected edge)."""
+
+    def __init__(self, size: int, adj: str):
+        if len(adj) < size * size:
+            raise ValueError("adjacency string shorter than size*size")
+        self.size = size
+        m = np.zeros((size, size), dtype=np.int32)
+        for i in range(size):
+            for j in range(size):
+                if adj[i * size + j] == "1":
+                    m[i, j] = m[j, i] = 1
+        self.adj = m
+
+    @property
+    def adj_string(self) -> str:
+        return "".join("1" if x else "0" for x in self.adj.reshape(-1))
+
+    @classmethod
+    def clique(cls, k: int) -> "Pattern":
+        return cls(k, "".join("0" if i == j else "1" for i in range(k) for j in range(k)))
+
+
+class Schedule_IEP:
+    """Immutable plan (reference include/schedule_IEP.h).  model=1 picks the
+    vertex order with the reference's analytic model from the graph's
+    v_cnt / e_cnt / tri_cnt; ``order``/``restricts`` give a schedule
+    explicitly; ``vertex_induced`` mirrors Schedule_IEP(adj_mat, size)."""
+
+    def __init__(self, pattern: Pattern, v_cnt: int = 0, e_cnt: int = 0, tri_cnt: int = 0, *,
+                 model: int = 1, enable_iep: bool = True, order: Optional[Sequence[int]] = None,
+                 restricts: Optional[Sequence[Sequence[int]]] = None, vertex_induced: bool = False):
+        L = lib()
+        h = C.c_void_p()
+        adj = pattern.adj_string.encode()
+        if vertex_induced:
+            check(L.gi_plan_create_induced(pattern.size, adj, C.byref(h)), "gi_plan_create_induced")
+        elif order is not None:
+            o = (C.c_int32 * pattern.size)(*order)
+            rs = list(restricts or [])
+            r = (C.c_int32 * max(1, 2 * len(rs)))(*[x for p in rs for x in p])
+            check(L.gi_plan_create_explicit(pattern.size, adj, o, r, len(rs), int(enable_iep), C.byref(h)),
+                  "gi_plan_create_explicit")
+        else:
+            check(L.gi_plan_create(pattern.size, adj, int(v_cnt), int(e_cnt), int(tri_cnt), int(model),
+                                   int(enable_iep), C.byref(h)), "gi_plan_create")
+        self._h = h
+        self.pattern = pattern
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            lib().gi_plan_destroy(h)
+            self._h = None
+
+    @property
+    def handle(self) -> C.c_void_p:
+        return self._h
+
+    def export(self) -> dict:
+        d = N.PlanDesc()
+        check(lib().gi_plan_export(self._h, C.byref(d)), "gi_plan_export")
+        n, tp = d.size, d.total_prefix_num
+        nr = d.total_restrict_num
+        out = {
+            "size": n,
+            "adj_mat": list(d.adj_mat[: n * n]),
+            "order": list(d.order[:n]),
+            "total_prefix_num": tp,
+            "basic_prefix_num": d.basic_prefix_num,
+            "father_prefix_id": list(d.father_prefix_id[:tp]),
+            "last": list(d.last[:n]),
+            "next": list(d.next[:tp]),
+            "loop_set_prefix_id": list(d.loop_set_prefix_id[:n]),
+            "break_size": list(d.break_size[:tp]),
+            "only_need_size": list(d.only_need_size[:tp]),
+            "prefix_data": [list(d.prefix_data[i][: d.prefix_len[i]]) for i in range(tp)],
+            "total_restrict_num": nr,
+            "restrict_last": list(d.restrict_last[:n]),
+            "restrict_next": list(d.restrict_next[:nr]),
+            "restrict_index": list(d.restrict_index[:nr]),
+            "restrict_pair": [list(d.restrict_pairs[i]) for i in range(d.n_restrict_pairs)],
+            "in_exclusion_optimize_num": d.in_exclusion_optimize_num,
+            "iep_vertex_id": list(d.iep_vertex_id[: d.iep_vertex_id_size]),
+            "iep_vertex_flag_eff": list(d.iep_vertex_flag[: d.iep_vertex_id_size]),
+            "iep_vertex_coef_eff": list(d.iep_vertex_coef[: d.iep_vertex_id_size]),
+            "iep_coef": list(d.iep_coef[: d.iep_term_count]),
+            "iep_flag": list(d.iep_flag[: d.iep_term_count]),
+            "iep_ans_pos_eff": list(d.iep_ans_pos[: d.iep_term_count]),
+            "is_vertex_induced": d.is_vertex_induced,
+            "redundancy": d.redundancy,
+            "k_val": d.k_val,
+            "multiplicity": d.multiplicity,
+            "model_cost": d.model_cost,
+            "iep_tables_rebuilt": d.iep_tables_rebuilt,
+            "count_divisor": d.count_divisor,
+            "exact": d.exact,
+        }
+        for which, key in ((0, "iep_vertex_flag"), (1, "iep_vertex_coef"), (2, "iep_ans_pos")):
+            n_raw = C.c_int64()
+            check(lib().gi_plan_export_raw(self._h, which, None, 0, C.byref(n_raw)), "gi_plan_export_raw")
+            buf = (C.c_int32 * max(1, n_raw.value))()
+            check(lib().gi_plan_export_raw(self._h, which, buf, n_raw.value, C.byref(n_raw)), "gi_plan_export_raw")
+            out[key] = list(buf[: n_raw.value])
+        return out
+
+    @staticmethod
+    def candidates(pattern: Pattern, v_cnt: int, e_cnt: int, tri_cnt: int, enable_iep: bool = True):
+        """(order, restricts, analytic cost, exact divisor or 0 if the
+        restriction set is invalid) in the reference model's order."""
+        L = lib()
+        adj = pattern.adj_string.encode()
+        cnt = C.c_int64()
+        check(L.gi_plan_candidates(pattern.size, adj, v_cnt, e_cnt, tri_cnt, int(enable_iep), None, None, None,
+                                   None, None, 0, C.byref(cnt)), "gi_plan_candidates")
+        m, n = cnt.value, pattern.size
+        orders = (C.c_int32 * max(1, m * n))()
+        rs = (C.c_int32 * max(1, m * N.GI_MAX_PREFIX * 2))()
+        nr = (C.c_int32 * max(1, m))()
+        costs = (C.c_double * max(1, m))()
+        divs = (C.c_int32 * max(1, m))()
+        check(L.gi_plan_candidates(pattern.size, adj, v_cnt, e_cnt, tri_cnt, int(enable_iep), orders, rs, nr,
+                                   costs, divs, m, C.byref(cnt)), "gi_plan_candidates")
+        out = []
+        for i in range(m):
+            r = [(rs[(i * N.GI_MAX_PREFIX + j) * 2], rs[(i * N.GI_MAX_PREFIX + j) * 2 + 1]) for j in range(nr[i])]
+            out.append((list(orders[i * n:(i + 1) * n]), r, costs[i], divs[i]))
+        return out
+
+
+@dataclass
+class CountResult:
+    count: int
+    kernel_ms: float
+    raw_sum: int
+    tasks: int
+    alg_bytes: int
+    grid_blocks: int
+    block_threads: int
+    kernel_launches: int
+
+
+def _stats(count_bytes: bool, budget_ms: float = 0.0) -> N.Stats:
+    s = N.Stats()
+    s.count_bytes = 1 if count_bytes else 0
+    s.budget_ms = float(budget_ms)
+    return s
+
+
+def _result(count: int, s: N.Stats) -> CountResult:
+    return CountResult(int(count), s.kernel_ms, int(s.raw_sum), int(s.tasks), int(s.alg_bytes), s.grid_blocks,
+                       s.block_threads, s.kernel_launches)
+
+
+class Graph:
+    """CSR graph resident on the current CUDA device (reference
+    include/graph.h:12-33).  ``vertex`` int64[v_cnt+1], ``edge`` int32[e_cnt]
+    with sorted, duplicate-free adjacency lists and both directions present."""
+
+    def __init__(self, handle: C.c_void_p):
+        self._h = handle
+        info = N.GraphInfo()
+        check(lib().gi_graph_get_info(handle, C.byref(info)), "gi_graph_get_info")
+        self.v_cnt = info.v_cnt
+        self.e_cnt = info.e_cnt
+        self.tri_cnt = info.tri_cnt
+        self.max_degree = info.max_degree
+        self.max_intersection_size = info.max_intersection_size
+
+    @classmethod
+    def from_csr(cls, vertex: np.ndarray, edge: np.ndarray, tri_cnt: int = 0, stream: int = 0) -> "Graph":
+        vertex = np.ascontiguousarray(vertex, dtype=np.int64)
+        edge = np.ascontiguousarray(edge, dtype=np.int32)
+        h = C.c_void_p()
+        check(lib().gi_graph_create(vertex.ctypes.data, edge.ctypes.data if edge.size else None,
+                                    len(vertex) - 1, len(edge), int(tri_cnt), C.c_void_p(stream) if stream else None,
+                                    C.byref(h)), "gi_graph_create")
+        return cls(h)
+
+    @classmethod
+    def load_g(cls, path: str) -> "Graph":
+        h = C.c_void_p()
+        check(lib().gi_graph_load_g(str(path).encode(), C.byref(h)), "gi_graph_load_g")
+        return cls(h)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            lib().gi_graph_destroy(h)
+            self._h = None
+
+    @property
+    def handle(self) -> C.c_void_p:
+        return self._h
+
+    def plan(self, pattern: Pattern, enable_iep: bool = True, model: int = 1) -> Schedule_IEP:
+        return Schedule_IEP(pattern, self.v_cnt, self.e_cnt, self.tri_cnt, model=model, enable_iep=enable_iep)
+
+
+def pattern_matching(graph: Graph, schedule: Schedule_IEP, *, count_bytes: bool = False, budget_ms: float = 0.0,
+                     stream: int = 0) -> CountResult:
+    """Count of the schedule's pattern (gpu_graph semantics: raw sum modulo
+    2^64 divided by the redundancy)."""
+    out = C.c_uint64()
+    s = _stats(count_bytes, budget_ms)
+    check(lib().gi_count(graph.handle, schedule.handle, C.c_void_p(stream) if stream else None, C.byref(out),
+                         C.byref(s)), "gi_count")
+    return _result(out.value, s)
+
+
+def clique_count(graph: Graph, k: int, orientation: int = 0, *, count_bytes: bool = False,
+                 stream: int = 0) -> CountResult:
+    out = C.c_uint64()
+    s = _stats(count_bytes)
+    check(lib().gi_clique_count(graph.handle, k, orientation, C.c_void_p(stream) if stream else None,
+                                C.byref(out), C.byref(s)), "gi_clique_count")
+    return _result(out.value, s)
+
+
+def motif_patterns(k: int) -> list[str]:
+    L = lib()
+    m = L.gi_motif_num(k)
+    if m < 0:
+        raise ValueError("motif size must be between 3 and 7")
+    buf = C.create_string_buffer(m * k * k)
+    check(L.gi_motif_patterns(k, buf, m), "gi_motif_patterns")
+    raw = buf.raw
+    return [raw[i * k * k:(i + 1) * k * k].decode() for i in range(m)]
+
+
+def motif_counting(graph: Graph, k: int, *, stream: int = 0) -> tuple[list[int], CountResult]:
+    L = lib()
+    m = L.gi_motif_num(k)
+    out = (C.c_uint64 * max(1, m))()
+    s = _stats(False)
+    check(L.gi_motif_count(graph.handle, k, C.c_void_p(stream) if stream else None, out, m, C.byref(s)),
+          "gi_motif_count")
+    return [int(x) for x in out[:m]], _result(0, s)
+
+
+def write_g(path: str, vertex: np.ndarray, edge: np.ndarray, max_isect: int, tri_cnt: int) -> None:
+    vertex = np.ascontiguousarray(vertex, dtype=np.int64)
+    edge = np.ascontiguousarray(edge, dtype=np.int32)
+    check(lib().gi_g_write(str(path).encode(), vertex.ctypes.data, edge.ctypes.data if edge.size else None,
+                           len(vertex) - 1, len(edge), int(max_isect), int(tri_cnt)), "gi_g_write")
+
+
+def read_g(path: str):
+    L = lib()
+    v, e, mi, tri = C.c_int32(), C.c_int64(), C.c_uint32(), C.c_int64()
+    check(L.gi_g_read_header(str(path).encode(), C.byref(v), C.byref(e), C.byref(mi), C.byref(tri)),
+          "gi_g_read_header")
+    vertex = np.empty(v.value + 1, dtype=np.int64)
+    edge = np.empty(max(1, e.value), dtype=np.int32)
+    check(L.gi_g_read(str(path).encode(), vertex.ctypes.data, edge.ctypes.data, v.value, e.value), "gi_g_read")
+    return vertex, edge[: e.value], int(mi.value), int(tri.value)

@@ -1,0 +1,83 @@
+// Shared definitions behind the C ABI (include/gi.h).
+#pragma once
+
+#include <cstdint>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/gi.h"
+#include "planner.hpp"
+
+namespace gi {
+
+// Records a failure message for gi_last_error() and returns the status.
+int fail(int status, const std::string &msg);
+
+// Per-prefix build mode used by the counting kernels.
+enum PrefixMode : int32_t {
+    kAlias = 0,        // father == -1: the set is N(v) itself, no copy
+    kMaterialize = 1,  // S_father ∩ N(v) written to the warp's scratch slot
+    kSizeOnly = 2,     // only |S_father ∩ N(v)| is ever read
+};
+
+// The plan as the device reads it: flat, fixed-size, passed by value as a
+// kernel parameter.  Built once per gi_plan from the Schedule_IEP arrays.
+struct DevPlan {
+    int32_t n;                  // pattern size
+    int32_t iep_k;              // in_exclusion_optimize_num (0 = no IEP tail)
+    int32_t total_prefix;
+    int32_t n_slots;            // materialised prefixes = scratch slots per warp
+    int32_t first_restricted;   // restrict_last[1] != -1: tasks need v1 < v0
+    int32_t vertex_induced;
+    int32_t father[GI_MAX_PREFIX];
+    int32_t next[GI_MAX_PREFIX];
+    int32_t break_size[GI_MAX_PREFIX];
+    int32_t mode[GI_MAX_PREFIX];
+    int32_t slot[GI_MAX_PREFIX];
+    int32_t last[GI_MAX_PATTERN + 1];
+    int32_t loop_set[GI_MAX_PATTERN + 1];
+    int32_t restrict_last[GI_MAX_PATTERN + 1];
+    int32_t restrict_next[GI_MAX_PREFIX];
+    int32_t restrict_index[GI_MAX_PREFIX];
+    int32_t adj[GI_MAX_PATTERN * GI_MAX_PATTERN];
+    int32_t iep_nsets;
+    int32_t iep_nterms;
+    int32_t iep_set[GI_MAX_IEP_SETS];
+    int32_t iep_set_flag[GI_MAX_IEP_SETS];
+    int32_t iep_set_coef[GI_MAX_IEP_SETS];
+    int32_t iep_coef[GI_MAX_IEP_TERMS];
+    int32_t iep_flag[GI_MAX_IEP_TERMS];
+    int32_t iep_pos[GI_MAX_IEP_TERMS];
+};
+
+}  // namespace gi
+
+struct gi_plan {
+    std::unique_ptr<gi::Schedule_IEP> sched;
+    gi::DevPlan dev;
+    int multiplicity = 0;
+    bool iep_tables_rebuilt = false;
+};
+
+// Implemented in device code (graph.cu / count.cu).
+struct gi_graph {
+    int device = 0;
+    int32_t v_cnt = 0;
+    int64_t e_cnt = 0;
+    int64_t tri_cnt = 0;
+    int32_t max_degree = 0;
+    int32_t max_isect = 0;
+    int64_t *d_vertex = nullptr;
+    int32_t *d_edge = nullptr;
+    uint32_t *d_edge_from = nullptr;
+    // Scratch for the counting kernels, grown on demand; counts on one graph
+    // handle are serialised by `mu`.
+    std::mutex mu;
+    void *d_scratch = nullptr;
+    size_t scratch_bytes = 0;
+    unsigned long long *d_counters = nullptr;  // [0] sum, [1] task cursor, [2] bytes, [3] tasks, ...
+    // Lazily built derived graphs (clique orientations).
+    gi_graph *oriented[2] = {nullptr, nullptr};
+};

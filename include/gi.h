@@ -1,0 +1,236 @@
+/*
+ * graphindor_b200 — C ABI of the B200 pattern-counting engine.
+ *
+ * The reference (GraphSet) has no library ABI: its surface is the host
+ * classes Pattern / Schedule_IEP / Graph and one kernel launch per pattern on
+ * a PatternMatchingDeviceContext (reference gpu/function/pattern_matching.cuh:
+ * 9-105, gpu/gpu_graph.cu:22-51).  These entry points replace that surface
+ * with plain pointers and sizes.  Every function returns a gi_status; none
+ * calls exit().  Distinct handles may be used from different threads; a graph
+ * handle serialises the counts that run on it.  Counts are uint64 and follow
+ * the reference GPU path's arithmetic: the per-embedding sum is taken modulo
+ * 2^64 and then divided by the plan's redundancy (reference
+ * gpu/gpu_graph.cu:42-44).
+ */
+#ifndef GRAPHINDOR_B200_GI_H
+#define GRAPHINDOR_B200_GI_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GI_MAX_PATTERN 7        /* reference MAX_DEPTH, gpu/function/pattern_matching.cuh:7 */
+#define GI_MAX_PREFIX 22        /* n(n-1)/2 + 1 for n = 7 */
+#define GI_MAX_IEP_SETS 32      /* distinct IEP sets for a 5-vertex tail */
+#define GI_MAX_IEP_TERMS 160    /* blocks over all set partitions of 5 (151) */
+
+typedef enum gi_status {
+    GI_OK = 0,
+    GI_EINVAL = 1,       /* bad argument, pattern too large, bad adjacency string */
+    GI_ENOMEM = 2,       /* host or device allocation failed */
+    GI_ECUDA = 3,        /* a CUDA call failed; see gi_last_error() */
+    GI_ETIMEOUT = 4,     /* a device work budget ran out before the count finished */
+    GI_EOVERFLOW = 5,    /* a size does not fit the engine's index types */
+    GI_EIO = 6,          /* file missing, short read, bad .g checksum */
+    GI_ENOTSUP = 7,      /* option not supported by this build */
+    GI_EDISCONNECTED = 8 /* pattern is not connected (reference throws) */
+} gi_status;
+
+typedef struct gi_graph gi_graph;           /* CSR resident on one GPU */
+typedef struct gi_plan gi_plan;             /* immutable Schedule_IEP */
+typedef struct gi_labeled_graph gi_labeled_graph;
+typedef void *gi_stream;                    /* a cudaStream_t; NULL = legacy default stream */
+
+/* Human-readable text of a status, and of the calling thread's last failure. */
+const char *gi_status_string(int status);
+const char *gi_last_error(void);
+int gi_version(void);
+
+/* ------------------------------------------------------------------ graph */
+
+/* Replaces Graph + PatternMatchingDeviceContext::init's CSR upload
+ * (reference include/graph.h:12-33, gpu/function/pattern_matching.cuh:18-81).
+ * vertex[v_cnt+1] int64 offsets, edge[e_cnt] int32 sorted adjacency, e_cnt =
+ * directed entries (twice the undirected edges).  The library copies both
+ * arrays to the current device on `stream` and owns the copy.  tri_cnt feeds
+ * the analytic planner only. */
+int gi_graph_create(const int64_t *vertex, const int32_t *edge, int32_t v_cnt, int64_t e_cnt,
+                    int64_t tri_cnt, gi_stream stream, gi_graph **out);
+/* Replaces DataLoader::fast_load (reference src/dataloader.cpp:78-124). */
+int gi_graph_load_g(const char *path, gi_graph **out);
+int gi_graph_destroy(gi_graph *g);
+
+typedef struct gi_graph_info {
+    int32_t v_cnt;
+    int64_t e_cnt;
+    int64_t tri_cnt;
+    int32_t max_degree;
+    int32_t max_intersection_size; /* second-largest degree (reference src/dataloader.cpp:297-301) */
+} gi_graph_info;
+int gi_graph_get_info(const gi_graph *g, gi_graph_info *out);
+
+/* --------------------------------------------------------- .g file format */
+/* 32-byte header {i32 v_cnt, 4 pad, i64 e_cnt, u32 max_intersection_size,
+ * u32 checksum, i64 tri_cnt}; the header's 32-bit words sum to zero
+ * (reference src/dataloader.cpp:21-47).  Host only, no GPU needed. */
+int gi_g_write(const char *path, const int64_t *vertex, const int32_t *edge, int32_t v_cnt, int64_t e_cnt,
+               uint32_t max_intersection_size, int64_t tri_cnt);
+int gi_g_read_header(const char *path, int32_t *v_cnt, int64_t *e_cnt, uint32_t *max_intersection_size,
+                     int64_t *tri_cnt);
+/* Reads the arrays into caller buffers of at least v_cnt+1 / e_cnt entries. */
+int gi_g_read(const char *path, int64_t *vertex, int32_t *edge, int32_t v_cap, int64_t e_cap);
+
+/* ------------------------------------------------------------------- plan */
+
+/* Replaces Schedule_IEP(Pattern(n, adj), valid, model, 1, enable_iep, v_cnt,
+ * e_cnt, tri_cnt) (reference include/schedule_IEP.h:15-18,
+ * src/schedule_IEP.cpp:12-247; gpu/gpu_graph.cu:102).  model 1 = the
+ * reference's analytic model, 0 = keep the pattern's own order: both give
+ * the reference's plan, and its count, bit for bit.  model 2 = the same
+ * analytic model over the candidates whose restriction set is valid (every
+ * subgraph passes its restrictions equally often), divided by that exact
+ * multiplicity: an exact count even for patterns where the reference's own
+ * restriction generator picks an invalid set.  Returns
+ * GI_EDISCONNECTED for a disconnected pattern and GI_EINVAL for n outside
+ * [3, 7] or an adjacency string shorter than n*n. */
+int gi_plan_create(int n, const char *adj, int32_t v_cnt, int64_t e_cnt, int64_t tri_cnt, int model,
+                   int enable_iep, gi_plan **out);
+/* A candidate schedule given explicitly: order[i] is the pattern vertex at
+ * position i; restricts holds n_restricts (first, second) position pairs
+ * meaning id(position second) < id(position first).  The count is exact:
+ * GI_EINVAL if the restriction set counts some subgraphs more often than
+ * others. */
+int gi_plan_create_explicit(int n, const char *adj, const int32_t *order, const int32_t *restricts,
+                            int n_restricts, int enable_iep, gi_plan **out);
+/* Replaces Schedule_IEP(adj_mat, size): vertex-induced, given order, no
+ * restrictions, no IEP (reference src/schedule_IEP.cpp:249-290). */
+int gi_plan_create_induced(int n, const char *adj, gi_plan **out);
+int gi_plan_destroy(gi_plan *p);
+
+/* A POD mirror of the Schedule_IEP arrays (reference include/schedule_IEP.h
+ * :30-110).  The iep_vertex_flag / iep_vertex_coef / iep_ans_pos arrays hold
+ * the entries the reference reads (the first iep_vertex_id_size /
+ * iep_term_count entries of vectors it never clears between candidate
+ * orders); *_raw_len give those vectors' full lengths. */
+typedef struct gi_plan_desc {
+    int32_t size;
+    int32_t adj_mat[GI_MAX_PATTERN * GI_MAX_PATTERN];
+    int32_t order[GI_MAX_PATTERN];
+    int32_t total_prefix_num;
+    int32_t basic_prefix_num;
+    int32_t father_prefix_id[GI_MAX_PREFIX];
+    int32_t last[GI_MAX_PATTERN];
+    int32_t next[GI_MAX_PREFIX];
+    int32_t loop_set_prefix_id[GI_MAX_PATTERN];
+    int32_t break_size[GI_MAX_PREFIX];
+    int32_t only_need_size[GI_MAX_PREFIX];
+    int32_t prefix_len[GI_MAX_PREFIX];
+    int32_t prefix_data[GI_MAX_PREFIX][GI_MAX_PATTERN];
+    int32_t total_restrict_num;
+    int32_t restrict_last[GI_MAX_PATTERN];
+    int32_t restrict_next[GI_MAX_PREFIX];
+    int32_t restrict_index[GI_MAX_PREFIX];
+    int32_t n_restrict_pairs;
+    int32_t restrict_pairs[GI_MAX_PREFIX][2];
+    int32_t in_exclusion_optimize_num;
+    int32_t iep_vertex_id_size;
+    int32_t iep_vertex_id[GI_MAX_IEP_SETS];
+    int32_t iep_vertex_flag[GI_MAX_IEP_SETS];
+    int32_t iep_vertex_coef[GI_MAX_IEP_SETS];
+    int32_t iep_term_count;
+    int32_t iep_coef[GI_MAX_IEP_TERMS];
+    int32_t iep_flag[GI_MAX_IEP_TERMS];
+    int32_t iep_ans_pos[GI_MAX_IEP_TERMS];
+    int64_t iep_vertex_flag_raw_len;
+    int64_t iep_ans_pos_raw_len;
+    int32_t is_vertex_induced;
+    int64_t redundancy;
+    int32_t k_val;
+    int32_t multiplicity;
+    double model_cost;
+    int32_t iep_tables_rebuilt; /* 1 when the reference's own tables for this plan index
+                                   past its IEP set list (an out-of-bounds read there) and
+                                   the engine rebuilt them from the same order and
+                                   restrictions */
+    int64_t count_divisor;      /* the raw sum is divided by this: the redundancy for
+                                   reference plans, the exact multiplicity otherwise */
+    int32_t exact;              /* 1: the restrictions the DFS applies count every subgraph
+                                   exactly count_divisor times, so the count is the true
+                                   subgraph count; 0: they do not (the reference's restriction
+                                   generator picked an invalid set; the count still equals the
+                                   reference's); -1: vertex-induced plan, not checked */
+} gi_plan_desc;
+int gi_plan_export(const gi_plan *p, gi_plan_desc *out);
+/* Full never-cleared vectors: which = 0 vertex_flag, 1 vertex_coef,
+ * 2 ans_pos.  Copies up to cap entries, returns the length in *len. */
+int gi_plan_export_raw(const gi_plan *p, int which, int32_t *buf, int64_t cap, int64_t *len);
+
+/* Candidate (order, restriction set, analytic cost) triples in the order the
+ * reference model scores them (reference src/schedule_IEP.cpp:67-177).  Pass
+ * orders = NULL to query the count.  orders: cap*n ints; restricts: cap*
+ * GI_MAX_PREFIX*2 ints; n_restricts, costs, divisors: cap entries (divisor 0
+ * marks a restriction set that does not count every subgraph equally). */
+int gi_plan_candidates(int n, const char *adj, int32_t v_cnt, int64_t e_cnt, int64_t tri_cnt, int enable_iep,
+                       int32_t *orders, int32_t *restricts, int32_t *n_restricts, double *costs,
+                       int32_t *divisors, int64_t cap, int64_t *count);
+
+/* --------------------------------------------------------------- counting */
+
+typedef struct gi_stats {
+    double kernel_ms;        /* device time of the counting kernel(s), CUDA events */
+    uint64_t raw_sum;        /* sum before the division by redundancy (mod 2^64) */
+    uint64_t tasks;          /* first-level edge tasks that passed the depth-1 filters */
+    uint64_t alg_bytes;      /* algorithmic bytes, filled when count_bytes != 0 */
+    int32_t count_bytes;     /* in: 1 = run the instrumented kernel that also sums alg_bytes */
+    double budget_ms;        /* in: > 0 = stop claiming work after this much device time and
+                                return GI_ETIMEOUT (checked between tasks, never a wait) */
+    int32_t grid_blocks;     /* out: persistent blocks launched */
+    int32_t block_threads;   /* out */
+    int32_t kernel_launches; /* out: kernels of this library launched by the call */
+} gi_stats;
+
+/* Replaces gpu_pattern_matching<<<...>>> + the D2H of dev_sum + the
+ * division by redundancy (reference gpu/gpu_graph.cu:22-51,
+ * gpu/src/gpu_pattern_matching.cuh:14-104).  Blocks until the count is on
+ * the host.  stats may be NULL. */
+int gi_count(const gi_graph *g, const gi_plan *p, gi_stream stream, uint64_t *out_count, gi_stats *stats);
+
+#define GI_TASK_CHUNK 32 /* consecutive first-level edges per claimed work item */
+
+/* Partial count over shard `shard` of `num_shards`.  First-level tasks (the
+ * directed edges) are grouped in chunks of GI_TASK_CHUNK consecutive edges;
+ * chunk c belongs to shard c % num_shards — the reference's static
+ * multi-device interleave (reference gpu/src/
+ * gpu_pattern_matching_static_task.cuh:63, driven per device by
+ * gpu/gpu_graph_static_task.cu).  *raw_sum receives the shard's sum modulo
+ * 2^64, not divided: the shards' sums add up (mod 2^64) to the whole
+ * graph's raw sum, which the caller divides by gi_plan_desc.count_divisor
+ * after reducing across devices.  stats->alg_bytes excludes the per-start-
+ * vertex depth-0 aliases that gi_count adds. */
+int gi_count_shard(const gi_graph *g, const gi_plan *p, int32_t shard, int32_t num_shards, gi_stream stream,
+                   uint64_t *raw_sum, gi_stats *stats);
+
+/* Replaces gpu_clique (reference gpu/gpu_clique.cu:573-639) when
+ * orientation = 0: k-cliques on the id-oriented DAG (keep u < v,
+ * reference src/graph.cpp:710-735); and gpu_kclique (reference
+ * gpu/gpu_kclique.cu:517-546) when orientation = 1: degree orientation
+ * (reference src/graph.cpp:821-859).  3 <= k <= 7. */
+int gi_clique_count(const gi_graph *g, int k, int orientation, gi_stream stream, uint64_t *out_count,
+                    gi_stats *stats);
+
+/* Replaces gpu_mc (reference gpu/gpu_mc.cu:62-119): edge-induced counts of
+ * every connected k-vertex pattern in the reference MotifGenerator order
+ * (reference src/motif_generator.cpp:5-43).  out_counts needs room for
+ * gi_motif_num(k) entries; adj_out (optional) receives k*k chars per motif. */
+int gi_motif_num(int k);
+int gi_motif_patterns(int k, char *adj_out, int cap);
+int gi_motif_count(const gi_graph *g, int k, gi_stream stream, uint64_t *out_counts, int cap, gi_stats *stats);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GRAPHINDOR_B200_GI_H */

@@ -1,0 +1,417 @@
+/*
+ * ORACLE — test infrastructure only (see oracle.h).  Plain C11 + OpenMP.
+ *
+ * oracle_count restates the reference CPU path:
+ *   Graph::pattern_matching             reference src/graph.cpp:305-355
+ *   Graph::pattern_matching_aggressive_func           src/graph.cpp:429-566
+ *   Graph::remove_anti_edge_vertices                  src/graph.cpp:195-232
+ *   VertexSet::build_vertex_set / intersection        src/vertex_set.cpp:83-91,203-215
+ *   VertexSet::unordered_subtraction_size             src/vertex_set.cpp:264-277
+ * on the plan arrays of a gi_plan_desc (the Schedule_IEP fields).
+ *
+ * Algorithmic bytes (counted when asked), per the engine's measurement
+ * definition, on this traversal:
+ *   materialised S_f ∩ N(v):      4 * (|S_f| + d(v) + |result|)
+ *   size-only S_f ∩ N(v):         4 * (|S_f| + d(v))
+ *   alias of N(v) (no father):    16
+ *   last-level count:             4 * size_after_restrict
+ *   IEP tail:                     4 * |S| for every set whose size alone is not enough
+ * where "size-only" marks a prefix with no child, not walked as a loop set
+ * before the IEP tail or the last position, and not needed by the IEP tail
+ * as members.
+ */
+#include "oracle.h"
+
+#include <omp.h>
+#include <stdlib.h>
+#include <string.h>
+
+typedef struct {
+    const gi_plan_desc *P;
+    const int64_t *vertex;
+    const int32_t *edge;
+    int32_t v_cnt;
+    int n, k;
+    int32_t *buf[GI_MAX_PREFIX];
+    int32_t *diff[GI_MAX_PATTERN + 1];
+    const int32_t *ptr[GI_MAX_PREFIX];
+    int32_t size[GI_MAX_PREFIX];
+    int size_only[GI_MAX_PREFIX];
+    int32_t emb[GI_MAX_PATTERN + 1];
+    int depth_emb;
+    int ans[GI_MAX_IEP_SETS];
+    uint64_t sum;
+    uint64_t bytes;
+    int want_bytes;
+} dfs_t;
+
+static int lower_bound_i32(const int32_t *a, int n, int32_t x) {
+    int lo = 0, hi = n;
+    while (lo < hi) {
+        int mid = (lo + hi) >> 1;
+        if (a[mid] < x) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+
+static int contains_i32(const int32_t *a, int n, int32_t x) {
+    int i = lower_bound_i32(a, n, x);
+    return i < n && a[i] == x;
+}
+
+/* |set0[0, size0) - emb[0, d)| — reference src/vertex_set.cpp:264-277 */
+static int subtraction_size(const int32_t *set0, int size0, const int32_t *emb, int d) {
+    int ret = size0;
+    for (int j = 0; j < d; ++j)
+        if (contains_i32(set0, size0, emb[j])) --ret;
+    return ret;
+}
+
+static int merge_intersect(const int32_t *a, int na, const int32_t *b, int nb, int32_t *out) {
+    int i = 0, j = 0, c = 0;
+    while (i < na && j < nb) {
+        if (a[i] < b[j]) ++i;
+        else if (a[i] > b[j]) ++j;
+        else {
+            out[c++] = a[i];
+            ++i;
+            ++j;
+        }
+    }
+    return c;
+}
+
+/* reference src/vertex_set.cpp:203-215: father -1 aliases N(v), otherwise
+ * S_father ∩ N(v). */
+static void build_vertex_set(dfs_t *s, int p, int32_t v) {
+    const int64_t l = s->vertex[v], r = s->vertex[v + 1];
+    const int32_t *nb = s->edge + l;
+    const int deg = (int)(r - l);
+    const int f = s->P->father_prefix_id[p];
+    if (f == -1) {
+        s->ptr[p] = nb;
+        s->size[p] = deg;
+        if (s->want_bytes) s->bytes += 16;
+    } else {
+        const int fn = s->size[f];
+        const int c = merge_intersect(s->ptr[f], fn, nb, deg, s->buf[p]);
+        s->ptr[p] = s->buf[p];
+        s->size[p] = c;
+        if (s->want_bytes) s->bytes += 4ull * (uint64_t)(fn + deg + (s->size_only[p] ? 0 : c));
+    }
+}
+
+/* reference src/graph.cpp:195-232 */
+static int remove_anti_edge(dfs_t *s, const int32_t *in, int n_in, int32_t *out, int vp) {
+    int c = 0;
+    const int n = s->n;
+    for (int i = 0; i < n_in; ++i) {
+        int keep = 1;
+        for (int u = 0; u < vp && keep; ++u) {
+            if (s->P->adj_mat[u * n + vp]) continue;
+            const int32_t v = s->emb[u];
+            const int64_t l = s->vertex[v], r = s->vertex[v + 1];
+            if (contains_i32(s->edge + l, (int)(r - l), in[i])) keep = 0;
+        }
+        if (keep) out[c++] = in[i];
+    }
+    return c;
+}
+
+static int has_data(const dfs_t *s, int d, int32_t v) {
+    for (int i = 0; i < d; ++i)
+        if (s->emb[i] == v) return 1;
+    return 0;
+}
+
+/* reference src/graph.cpp:429-566 */
+static void aggressive(dfs_t *s, int depth) {
+    const gi_plan_desc *P = s->P;
+    const int n = s->n, k = s->k;
+    const int ls = P->loop_set_prefix_id[depth];
+    const int32_t *vset = s->ptr[ls];
+    int loop_size = s->size[ls];
+    if (loop_size <= 0) return;
+    if (P->is_vertex_induced) {
+        loop_size = remove_anti_edge(s, vset, loop_size, s->diff[depth], depth);
+        vset = s->diff[depth];
+    }
+    if (depth == n - k) {
+        /* IEP tail, reference src/graph.cpp:456-493 */
+        for (int i = 0; i < P->iep_vertex_id_size; ++i) {
+            const int p = P->iep_vertex_id[i];
+            if (P->iep_vertex_flag[i]) {
+                s->ans[i] = s->size[p] - P->iep_vertex_coef[i];
+            } else {
+                s->ans[i] = subtraction_size(s->ptr[p], s->size[p], s->emb, depth);
+                if (s->want_bytes) s->bytes += 4ull * (uint64_t)s->size[p];
+            }
+        }
+        int last_pos = -1;
+        uint64_t val = 0;
+        for (int pos = 0; pos < P->iep_term_count; ++pos) {
+            const int64_t a = s->ans[P->iep_ans_pos[pos]];
+            if (pos == last_pos + 1) val = (uint64_t)a;
+            else if (val != 0) val = val * (uint64_t)a;
+            if (P->iep_flag[pos]) {
+                last_pos = pos;
+                s->sum += val * (uint64_t)(int64_t)P->iep_coef[pos];
+            }
+        }
+        return;
+    }
+    if (depth == n - 1) {
+        int size_after = loop_size;
+        if (P->total_restrict_num > 0) {
+            int32_t min_vertex = s->v_cnt;
+            for (int i = P->restrict_last[depth]; i != -1; i = P->restrict_next[i])
+                if (min_vertex > s->emb[P->restrict_index[i]]) min_vertex = s->emb[P->restrict_index[i]];
+            size_after = lower_bound_i32(vset, loop_size, min_vertex);
+        }
+        if (s->want_bytes) s->bytes += 4ull * (uint64_t)size_after;
+        if (size_after > 0) s->sum += (uint64_t)(int64_t)subtraction_size(vset, size_after, s->emb, depth);
+        return;
+    }
+    int32_t min_vertex = s->v_cnt;
+    for (int i = P->restrict_last[depth]; i != -1; i = P->restrict_next[i])
+        if (min_vertex > s->emb[P->restrict_index[i]]) min_vertex = s->emb[P->restrict_index[i]];
+    for (int i = 0; i < loop_size; ++i) {
+        const int32_t v = vset[i];
+        if (min_vertex <= v) break;
+        if (has_data(s, depth, v)) continue;
+        int zero = 0;
+        for (int p = P->last[depth]; p != -1; p = P->next[p]) {
+            build_vertex_set(s, p, v);
+            if (s->size[p] == P->break_size[p]) {
+                zero = 1;
+                break;
+            }
+        }
+        if (zero) continue;
+        s->emb[depth] = v;
+        aggressive(s, depth + 1);
+    }
+}
+
+static void classify(const gi_plan_desc *P, int *size_only) {
+    const int tp = P->total_prefix_num, n = P->size, k = P->in_exclusion_optimize_num;
+    int need[GI_MAX_PREFIX] = {0};
+    for (int p = 0; p < tp; ++p)
+        if (P->father_prefix_id[p] >= 0) need[P->father_prefix_id[p]] = 1;
+    const int end = k > 0 ? n - k : n;
+    for (int d = 1; d < end; ++d)
+        if (P->loop_set_prefix_id[d] >= 0) need[P->loop_set_prefix_id[d]] = 1;
+    for (int i = 0; i < P->iep_vertex_id_size && k > 0; ++i)
+        if (!P->iep_vertex_flag[i]) need[P->iep_vertex_id[i]] = 1;
+    for (int p = 0; p < tp; ++p) size_only[p] = P->father_prefix_id[p] >= 0 && !need[p];
+}
+
+int oracle_count(const gi_plan_desc *P, const int64_t *vertex, const int32_t *edge, int32_t v_cnt,
+                 int32_t v_begin, int32_t v_end, int threads, uint64_t *raw_sum, uint64_t *alg_bytes) {
+    if (!P || !vertex || !raw_sum || P->size < 3 || P->size > GI_MAX_PATTERN || v_cnt < 1) return -1;
+    if (v_begin < 0) v_begin = 0;
+    if (v_end > v_cnt) v_end = v_cnt;
+    int max_deg = 1;
+    for (int32_t v = 0; v < v_cnt; ++v) {
+        const int d = (int)(vertex[v + 1] - vertex[v]);
+        if (d > max_deg) max_deg = d;
+    }
+    uint64_t total = 0, total_bytes = 0;
+    int size_only[GI_MAX_PREFIX];
+    classify(P, size_only);
+    if (threads <= 0) threads = omp_get_max_threads();
+#pragma omp parallel num_threads(threads) reduction(+ : total, total_bytes)
+    {
+        dfs_t s;
+        memset(&s, 0, sizeof(s));
+        s.P = P;
+        s.vertex = vertex;
+        s.edge = edge;
+        s.v_cnt = v_cnt;
+        s.n = P->size;
+        s.k = P->in_exclusion_optimize_num;
+        s.want_bytes = alg_bytes != NULL;
+        memcpy(s.size_only, size_only, sizeof(size_only));
+        for (int p = 0; p < P->total_prefix_num; ++p) s.buf[p] = (int32_t *)malloc(sizeof(int32_t) * (size_t)max_deg);
+        for (int d = 0; d <= GI_MAX_PATTERN; ++d) s.diff[d] = (int32_t *)malloc(sizeof(int32_t) * (size_t)max_deg);
+#pragma omp for schedule(dynamic, 16) nowait
+        for (int32_t v = v_begin; v < v_end; ++v) {
+            for (int p = P->last[0]; p != -1; p = P->next[p]) build_vertex_set(&s, p, v);
+            s.emb[0] = v;
+            aggressive(&s, 1);
+        }
+        total += s.sum;
+        total_bytes += s.bytes;
+        for (int p = 0; p < P->total_prefix_num; ++p) free(s.buf[p]);
+        for (int d = 0; d <= GI_MAX_PATTERN; ++d) free(s.diff[d]);
+    }
+    *raw_sum = total;
+    if (alg_bytes) *alg_bytes = total_bytes;
+    return 0;
+}
+
+/* ------------------------------------------------------------ brute force */
+
+static int adjacent(const int64_t *vertex, const int32_t *edge, int32_t a, int32_t b) {
+    return contains_i32(edge + vertex[a], (int)(vertex[a + 1] - vertex[a]), b);
+}
+
+typedef struct {
+    int n, induced;
+    int adj[GI_MAX_PATTERN * GI_MAX_PATTERN];
+    int order[GI_MAX_PATTERN];   /* pattern vertices in BFS order */
+    int anchor[GI_MAX_PATTERN];  /* an earlier BFS neighbour, -1 for the root */
+    const int64_t *vertex;
+    const int32_t *edge;
+    int32_t v_cnt;
+    int32_t map[GI_MAX_PATTERN];
+    uint64_t count;
+} brute_t;
+
+static void brute_rec(brute_t *b, int i) {
+    if (i == b->n) {
+        ++b->count;
+        return;
+    }
+    const int pv = b->order[i];
+    const int32_t *cand;
+    int nc;
+    int32_t all_dummy = 0;
+    if (b->anchor[i] < 0) {
+        cand = NULL;
+        nc = b->v_cnt;
+    } else {
+        const int32_t a = b->map[b->anchor[i]];
+        cand = b->edge + b->vertex[a];
+        nc = (int)(b->vertex[a + 1] - b->vertex[a]);
+    }
+    (void)all_dummy;
+    for (int c = 0; c < nc; ++c) {
+        const int32_t x = cand ? cand[c] : c;
+        int ok = 1;
+        for (int j = 0; j < i && ok; ++j) {
+            const int qv = b->order[j];
+            const int32_t y = b->map[qv];
+            if (y == x) ok = 0;
+            else if (b->adj[pv * b->n + qv]) ok = adjacent(b->vertex, b->edge, x, y);
+            else if (b->induced) ok = !adjacent(b->vertex, b->edge, x, y);
+        }
+        if (!ok) continue;
+        b->map[pv] = x;
+        brute_rec(b, i + 1);
+    }
+}
+
+static uint64_t automorphisms(int n, const int *adj) {
+    int p[GI_MAX_PATTERN], c[GI_MAX_PATTERN] = {0};
+    for (int i = 0; i < n; ++i) p[i] = i;
+    uint64_t count = 0;
+    /* Heap's algorithm over all n! permutations. */
+    int i = 0;
+    for (;;) {
+        int ok = 1;
+        for (int a = 0; a < n && ok; ++a)
+            for (int b = 0; b < n; ++b)
+                if (adj[a * n + b] != adj[p[a] * n + p[b]]) {
+                    ok = 0;
+                    break;
+                }
+        count += (uint64_t)ok;
+        while (i < n && c[i] >= i) c[i++] = 0;
+        if (i >= n) break;
+        if (i % 2 == 0) {
+            int t = p[0]; p[0] = p[i]; p[i] = t;
+        } else {
+            int t = p[c[i]]; p[c[i]] = p[i]; p[i] = t;
+        }
+        ++c[i];
+        i = 0;
+    }
+    return count;
+}
+
+uint64_t oracle_brute_count(int n, const char *adj, int induced, const int64_t *vertex, const int32_t *edge,
+                            int32_t v_cnt) {
+    brute_t b;
+    memset(&b, 0, sizeof(b));
+    b.n = n;
+    b.induced = induced;
+    b.vertex = vertex;
+    b.edge = edge;
+    b.v_cnt = v_cnt;
+    for (int i = 0; i < n * n; ++i) b.adj[i] = adj[i] == '1';
+    for (int i = 0; i < n; ++i)
+        for (int j = 0; j < n; ++j)
+            if (b.adj[i * n + j]) b.adj[j * n + i] = 1;
+    int seen[GI_MAX_PATTERN] = {0};
+    int cnt = 0;
+    b.order[cnt] = 0;
+    b.anchor[cnt++] = -1;
+    seen[0] = 1;
+    for (int h = 0; h < cnt; ++h)
+        for (int j = 0; j < n; ++j)
+            if (b.adj[b.order[h] * n + j] && !seen[j]) {
+                seen[j] = 1;
+                b.anchor[cnt] = b.order[h];
+                b.order[cnt++] = j;
+            }
+    if (cnt != n) return 0; /* disconnected patterns are rejected by the engine */
+    brute_rec(&b, 0);
+    return b.count / automorphisms(n, b.adj);
+}
+
+static uint64_t clique_rec(const int64_t *vertex, const int32_t *edge, int32_t *pick, int depth, int k,
+                           int32_t v_cnt) {
+    if (depth == k) return 1;
+    uint64_t c = 0;
+    const int32_t last = pick[depth - 1];
+    for (int64_t e = vertex[last]; e < vertex[last + 1]; ++e) {
+        const int32_t x = edge[e];
+        if (x <= last) continue;
+        int ok = 1;
+        for (int j = 0; j < depth - 1 && ok; ++j) ok = adjacent(vertex, edge, x, pick[j]);
+        if (!ok) continue;
+        pick[depth] = x;
+        c += clique_rec(vertex, edge, pick, depth + 1, k, v_cnt);
+    }
+    return c;
+}
+
+uint64_t oracle_clique_count(int k, const int64_t *vertex, const int32_t *edge, int32_t v_cnt) {
+    uint64_t total = 0;
+    int32_t pick[GI_MAX_PATTERN + 1];
+    if (k < 1 || k > GI_MAX_PATTERN) return 0;
+    for (int32_t v = 0; v < v_cnt; ++v) {
+        pick[0] = v;
+        total += clique_rec(vertex, edge, pick, 1, k, v_cnt);
+    }
+    return total;
+}
+
+uint64_t oracle_triangles(const int64_t *vertex, const int32_t *edge, int32_t v_cnt, int threads) {
+    uint64_t total = 0;
+    if (threads <= 0) threads = omp_get_max_threads();
+#pragma omp parallel for num_threads(threads) schedule(dynamic, 64) reduction(+ : total)
+    for (int32_t v = 0; v < v_cnt; ++v) {
+        for (int64_t e = vertex[v]; e < vertex[v + 1]; ++e) {
+            const int32_t u = edge[e];
+            if (u >= v) break;
+            /* w < u < v, w in N(u) ∩ N(v) */
+            int64_t i = vertex[v], j = vertex[u];
+            const int64_t ie = vertex[v + 1], je = vertex[u + 1];
+            while (i < ie && j < je) {
+                const int32_t a = edge[i], b = edge[j];
+                if (a >= u || b >= u) break;
+                if (a < b) ++i;
+                else if (a > b) ++j;
+                else {
+                    ++total;
+                    ++i;
+                    ++j;
+                }
+            }
+        }
+    }
+    return total;
+}

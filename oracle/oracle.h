@@ -1,0 +1,54 @@
+/*
+ * ORACLE — test infrastructure only.
+ *
+ * A plain-C restatement of the reference's CPU counting path, used by tests/,
+ * the smoke check and bench.py's CPU-baseline leg to check and time the CUDA
+ * engine.  Nothing in the engine links, loads or calls it.
+ *
+ * Parity is pinned by tests against (a) the reference's own binaries built
+ * from its sources by oracle/Makefile (counts on seeded graphs, committed
+ * under tests/golden/) and (b) the reference's published triangle count for
+ * Wiki-Vote and the survey-measured Wiki-Vote pattern counts.
+ */
+#ifndef GI_ORACLE_H
+#define GI_ORACLE_H
+
+#include <stdint.h>
+
+#include "../include/gi.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Count of the plan on the graph with the reference CPU path's semantics
+ * (reference src/graph.cpp:305-355 pattern_matching, :429-566
+ * pattern_matching_aggressive_func, src/vertex_set.cpp:203-277).  Start
+ * vertices v0 in [v_begin, v_end) only (the whole graph: 0, v_cnt), run over
+ * `threads` OpenMP threads (0 = all).  *raw_sum receives the sum before the
+ * division by redundancy, modulo 2^64.  If alg_bytes is non-NULL it receives
+ * the algorithmic bytes of the traversal (see oracle.c).  Returns 0, or -1
+ * on bad input. */
+int oracle_count(const gi_plan_desc *plan, const int64_t *vertex, const int32_t *edge, int32_t v_cnt,
+                 int32_t v_begin, int32_t v_end, int threads, uint64_t *raw_sum, uint64_t *alg_bytes);
+
+/* Independent brute force: number of subgraphs of the graph isomorphic to
+ * the n-vertex pattern adj (n*n '0'/'1'), edge-induced (induced = 0) or
+ * vertex-induced (induced = 1), as #injective maps / #automorphisms.  For
+ * small graphs only. */
+uint64_t oracle_brute_count(int n, const char *adj, int induced, const int64_t *vertex, const int32_t *edge,
+                            int32_t v_cnt);
+
+/* Number of k-cliques (undirected), by brute force over increasing vertex
+ * tuples.  For small graphs only. */
+uint64_t oracle_clique_count(int k, const int64_t *vertex, const int32_t *edge, int32_t v_cnt);
+
+/* Exact triangle count (each triangle once) by merging sorted lists,
+ * reference src/graph.cpp:1006-1043 (motif_counting_3). */
+uint64_t oracle_triangles(const int64_t *vertex, const int32_t *edge, int32_t v_cnt, int threads);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif
