@@ -1,0 +1,405 @@
+"""Benchmark: pattern counting with IEP on an R-MAT scale-22 graph, six patterns.
+
+Workload: a seeded R-MAT graph, scale 22 (4.19M vertices), edge factor 10.6
+(about 43M undirected edges once symmetrised, deduplicated and stripped of
+self-loops), a/b/c = 0.57/0.19/0.19, random relabelling; the six patterns
+diamond, 4-cycle, house, 5-clique, prism and 6-cycle with chord (0,3), each
+planned as the reference's gpu_graph plans them (analytic model, the
+reference's restriction generator, IEP on).
+
+The whole six-pattern job runs for hours, so the bench measures
+representative slices of it.  For pattern p, a slice is one shard of S_p:
+first-level subtasks are grouped in chunks and chunk c belongs to shard
+c mod S_p (the reference's static multi-device interleave), so every shard
+carries 1/S_p of the work, hubs included.  A step counts shard
+(step * world + rank) mod S_p of every pattern.
+
+value = whole-job throughput extrapolated from the slices:
+          sum_p (embeddings of p's shards) * S_p / sum_p (device time of p's shards) * S_p
+        with the graph resident in HBM (device time from CUDA events).
+e2e   = the same whole job through the public API from pinned host buffers:
+        graph upload (H2D) + planning + counts + result reads (D2H).
+cpu_baseline / --impl reference: the reference's CPU path (the oracle, a C
+        restatement of reference src/graph.cpp:305-566) on all host cores
+        over every s_p-th start vertex (an unbiased slice: ids are random),
+        extrapolated the same way.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+SCALE, EDGE_FACTOR, SEED = 22, 10.6, 2
+PATTERNS = [
+    ("diamond", 4, "0111101111001100"),
+    ("4-cycle", 4, "0110100110010110"),
+    ("house", 5, "0101110101010101010011000"),
+    ("5-clique", 5, "0111110111110111110111110"),
+    ("prism", 6, "011100101010110001100011010101001110"),
+    ("6-cycle+chord", 6, "010101101000010100101010000101100010"),
+]
+SHARDS: dict = {}           # pattern -> S_p (calibrated unless given with --shards)
+TARGET_SHARD_MS = 1000.0     # device time of one calibrated shard
+CPU_TARGET_S = 3.0           # host time of one pattern's CPU slice
+MEASURED = ROOT / "MEASURED_PEAKS.json"
+METRIC = "pattern-match embeddings/s, whole six-pattern job (R-MAT s22, IEP), 1 B200"
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--scale", type=int, default=SCALE)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--shards", default="", help="name=S,... fixes shard counts instead of calibrating")
+    ap.add_argument("--target-ms", type=float, default=TARGET_SHARD_MS)
+    ap.add_argument("--cpu-target-s", type=float, default=CPU_TARGET_S)
+    a = ap.parse_args()
+    for item in filter(None, a.shards.split(",")):
+        k, v = item.split("=")
+        SHARDS[k] = int(v)
+    return a
+
+
+def make_graph(scale: int):
+    from graphindor_b200 import gen
+    return gen.rmat(scale, EDGE_FACTOR, SEED)
+
+
+_PINNED = []  # keeps the pinned host buffers alive
+
+
+def pinned(a: np.ndarray) -> np.ndarray:
+    import torch
+    t = torch.empty(a.shape, dtype={np.int64: torch.int64, np.int32: torch.int32}[a.dtype.type], pin_memory=True)
+    _PINNED.append(t)
+    out = t.numpy()
+    out[...] = a
+    return out
+
+
+class Clocks:
+    """nvidia-smi samples (200 ms) taken during the timed region."""
+
+    def __init__(self, gpu_index: int):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={gpu_index}", f"--query-gpu={q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self) -> dict:
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        self.p.wait()
+        self.f.seek(0)
+        rows = [[x.strip() for x in r.split(",")] for r in self.f.read().splitlines() if r.strip()]
+        os.unlink(self.f.name)
+        num = lambda s: s.replace(".", "", 1).isdigit()  # noqa: E731
+        sm = [float(r[1]) for r in rows if len(r) >= 9 and num(r[1])]
+        mx = [float(r[2]) for r in rows if len(r) >= 9 and num(r[2])]
+        reasons = set()
+        for r in rows:
+            if len(r) < 9:
+                continue
+            for name, val in zip(["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"], r[5:9]):
+                if val == "Active":
+                    reasons.add(name)
+        busy = [x for x in sm if x > 500] or sm
+        return {"sm_mhz": statistics.median(busy) if busy else None, "sm_max_mhz": max(mx) if mx else None,
+                "samples": len(rows), "reasons": sorted(reasons)}
+
+
+def calibrate(L, N, graph, plans, sp, target_ms):
+    """Power-of-4 shard count per pattern whose shard 0 takes about target_ms."""
+    for name, _, _ in PATTERNS:
+        if name in SHARDS:
+            continue
+        S = 1 << 20
+        while True:
+            st = N.Stats()
+            st.budget_ms = 4.0 * target_ms
+            raw = C.c_uint64()
+            rc = L.gi_count_shard(graph.handle, plans[name].handle, 0, S, sp, C.byref(raw), C.byref(st))
+            if rc not in (N.GI_OK, N.GI_ETIMEOUT):
+                N.check(rc, "gi_count_shard")
+            if rc == N.GI_ETIMEOUT:
+                S = min(S * 4, 1 << 20)  # the previous, smaller shard
+                break
+            if st.kernel_ms >= target_ms / 4.0 or S == 1:
+                break
+            S //= 4
+        SHARDS[name] = max(1, S)
+
+
+def run_ours(args, world, rank, local):
+    import torch
+
+    import graphindor_b200 as gi
+    from graphindor_b200 import _native as N
+
+    torch.cuda.set_device(local)
+    L = gi.lib()
+    g = make_graph(args.scale)
+    vertex_h, edge_h = pinned(g.vertex), pinned(g.edge)
+    stream = torch.cuda.Stream()
+    sp = C.c_void_p(stream.cuda_stream)
+    dg = gi.Graph.from_csr(vertex_h, edge_h, stream=stream.cuda_stream)
+    tri = gi.clique_count(dg, 3, 1, stream=stream.cuda_stream).count  # the .g header's triangle count
+    del dg
+    dg = gi.Graph.from_csr(vertex_h, edge_h, tri_cnt=tri, stream=stream.cuda_stream)
+    plans = {name: gi.Schedule_IEP(gi.Pattern(n, adj), dg.v_cnt, dg.e_cnt, tri) for name, n, adj in PATTERNS}
+    divisors = {name: plans[name].export()["count_divisor"] for name, _, _ in PATTERNS}
+    calibrate(L, N, dg, plans, sp, args.target_ms)
+    if world > 1:
+        t = torch.tensor([SHARDS[name] for name, _, _ in PATTERNS], dtype=torch.int64, device="cuda")
+        torch.distributed.broadcast(t, 0)
+        for (name, _, _), s in zip(PATTERNS, t.tolist()):
+            SHARDS[name] = int(s)
+
+    def one_step(graph, plan_map, step, acc, count_bytes=False):
+        for name, _, _ in PATTERNS:
+            S = SHARDS[name]
+            st = N.Stats()
+            st.count_bytes = 1 if count_bytes else 0
+            raw = C.c_uint64()
+            N.check(L.gi_count_shard(graph.handle, plan_map[name].handle, (step * world + rank) % S, S, sp,
+                                     C.byref(raw), C.byref(st)), "gi_count_shard")
+            a = acc.setdefault(name, {"emb": 0.0, "ms": 0.0, "launches": 0, "bytes": 0})
+            a["emb"] += raw.value / divisors[name]
+            a["ms"] += st.kernel_ms
+            a["launches"] += st.kernel_launches
+            a["bytes"] += st.alg_bytes
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+
+    steps = range(args.warmup, args.warmup + args.steps)
+    for s in range(args.warmup):
+        one_step(dg, plans, s, {})
+    instr = {}
+    for s in steps:  # algorithmic bytes of the timed shards (instrumented pass, untimed)
+        one_step(dg, plans, s, instr, count_bytes=True)
+
+    clocks = Clocks(torch.cuda.current_device())
+    barrier()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    acc = {}
+    for s in steps:
+        one_step(dg, plans, s, acc)
+    ev1.record(stream)
+    barrier()
+    clk = clocks.stop()
+    dev_ms = ev0.elapsed_time(ev1)
+
+    # End to end through the public API, every step: upload from pinned host
+    # memory, planning, the shard counts, the result reads.
+    del dg
+    barrier()
+    e2e = {"upload_ms": 0.0, "plan_ms": 0.0}
+    e2e_acc = {}
+    for s in steps:
+        e0, e1, e2, e3 = (torch.cuda.Event(enable_timing=True) for _ in range(4))
+        e0.record(stream)
+        g2 = gi.Graph.from_csr(vertex_h, edge_h, tri_cnt=tri, stream=stream.cuda_stream)
+        e1.record(stream)
+        p2 = {name: gi.Schedule_IEP(gi.Pattern(n, adj), g2.v_cnt, g2.e_cnt, tri) for name, n, adj in PATTERNS}
+        e2.record(stream)
+        one_step(g2, p2, s, e2e_acc)
+        e3.record(stream)
+        e3.synchronize()
+        e2e["upload_ms"] += e0.elapsed_time(e1)
+        e2e["plan_ms"] += e1.elapsed_time(e2)
+        del g2, p2
+    barrier()
+
+    # Reduce over ranks: device times take the max, work adds up.
+    names = [n for n, _, _ in PATTERNS]
+    t_max = torch.tensor([dev_ms, e2e["upload_ms"], e2e["plan_ms"]] + [acc[n]["ms"] for n in names] +
+                         [e2e_acc[n]["ms"] for n in names], dtype=torch.float64, device="cuda")
+    w_sum = torch.tensor([acc[n]["emb"] for n in names] + [float(instr[n]["bytes"]) for n in names] +
+                         [float(acc[n]["launches"]) for n in names], dtype=torch.float64, device="cuda")
+    if world > 1:
+        torch.distributed.all_reduce(t_max, op=torch.distributed.ReduceOp.MAX)
+        torch.distributed.all_reduce(w_sum, op=torch.distributed.ReduceOp.SUM)
+    tm, ws = t_max.tolist(), w_sum.tolist()
+    k = len(names)
+    dev_ms, up_ms, plan_ms = tm[0], tm[1], tm[2]
+    ms_p, e2e_ms_p = dict(zip(names, tm[3:3 + k])), dict(zip(names, tm[3 + k:3 + 2 * k]))
+    emb_p, bytes_p, launch_p = (dict(zip(names, ws[i * k:(i + 1) * k])) for i in range(3))
+
+    job_emb = sum(emb_p[n] * SHARDS[n] for n in names)
+    job_ms = sum(ms_p[n] * SHARDS[n] for n in names)
+    # e2e whole job: one upload and one planning per job, the counts scaled
+    # from their shards.
+    job_e2e_ms = up_ms / args.steps + plan_ms / args.steps + sum(e2e_ms_p[n] * SHARDS[n] for n in names)
+
+    peaks = json.loads(MEASURED.read_text()) if MEASURED.exists() else {}
+    hbm = float(peaks.get("hbm_gbs", 6650.0))
+    total_bytes = sum(bytes_p.values())
+    count_ms = sum(ms_p.values())
+    achieved = total_bytes / world / (count_ms / 1e3) / 1e9 if count_ms else 0.0
+    line = {
+        "metric": METRIC,
+        "value": job_emb / (job_ms / 1e3),
+        "unit": "embeddings/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": dev_ms / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "u32 ids / u64 counts",
+        "data": "synthetic (seeded R-MAT, no dataset)",
+        "config": {
+            "workload": f"R-MAT scale {args.scale}, edge factor {EDGE_FACTOR}, seed {SEED}: {g.v_cnt} vertices, "
+                        f"{g.e_cnt // 2} undirected edges; six patterns with IEP, reference plans; whole-job "
+                        "throughput extrapolated from interleaved 1/S_p shards",
+            "patterns": {n: adj for n, _, adj in PATTERNS},
+            "shards": dict(SHARDS),
+            "per_pattern_job_s": {n: ms_p[n] * SHARDS[n] / 1e3 / args.steps for n in names},
+            "per_pattern_embeddings": {n: emb_p[n] * SHARDS[n] / args.steps for n in names},
+            "l2": "inputs larger than L2 (CSR %.2f GB vs 126 MB)" % ((g.vertex.nbytes + g.edge.nbytes) / 1e9),
+            "parallelism": f"dp{world}: shards interleaved across ranks",
+        },
+        "e2e": {"value": job_emb / (job_e2e_ms / 1e3), "unit": "embeddings/s",
+                "h2d_bytes_per_step": int(g.vertex.nbytes + g.edge.nbytes),
+                "d2h_bytes_per_step": int(2 * 64 * len(PATTERNS)),
+                "upload_ms_per_step": up_ms / args.steps, "plan_ms_per_step": plan_ms / args.steps},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                     "frac": achieved / hbm if hbm else None, "traffic": None, "kernel": "dfs_count_kernel",
+                     "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if MEASURED.exists() else "fallback",
+                     "note": "achieved = algorithmic bytes of the counting launches (merge-intersection "
+                             "accounting, counted by the instrumented kernel) / their CUDA-event time"},
+        "gpu_launches": int(sum(launch_p.values())),
+        "clocks": clk,
+    }
+    return line, g, plans, divisors
+
+
+def plan_descs(plans):
+    import graphindor_b200 as gi
+    from graphindor_b200 import _native as N
+    out = {}
+    for name, s in plans.items():
+        d = N.PlanDesc()
+        N.check(gi.lib().gi_plan_export(s.handle, C.byref(d)), "gi_plan_export")
+        out[name] = d
+    return out
+
+
+def cpu_job(g, descs, divisors, threads, target_s):
+    """The reference CPU path (oracle) on every s_p-th start vertex per
+    pattern, s_p the power of 4 whose slice takes about target_s; returns
+    (whole-job embeddings/s, sample text)."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle_py
+    job_emb = job_s = 0.0
+    parts = []
+    n = g.v_cnt
+    for name, _, _ in PATTERNS:
+        stride = 1 << 20
+        while True:
+            t0 = time.perf_counter()
+            # A slice never runs much past 2 * target_s: no start vertex is
+            # begun after that; the extrapolation uses those counted.
+            raw, done = oracle_py.count_timed(descs[name], g.vertex, g.edge, stride, 2.0 * target_s, threads)
+            dt = time.perf_counter() - t0
+            if dt >= target_s / 4.0 or stride == 1:
+                break
+            stride //= 4
+        scale = n / max(1, done)
+        job_emb += raw / divisors[name] * scale
+        job_s += dt * scale
+        parts.append(f"{name}: {done} start vertices (every {stride}th), {dt:.2f}s")
+    return job_emb / job_s if job_s else 0.0, "; ".join(parts)
+
+
+def run_reference(args, world):
+    """Reference arm: the reference's CPU path on all host cores."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle_py
+
+    import graphindor_b200 as gi
+    g = make_graph(args.scale)
+    tri = int(oracle_py.triangles(g.vertex, g.edge))
+    plans = {name: gi.Schedule_IEP(gi.Pattern(n, adj), g.v_cnt, g.e_cnt, tri) for name, n, adj in PATTERNS}
+    descs = plan_descs(plans)
+    divisors = {n: descs[n].count_divisor for n in descs}
+    threads = os.cpu_count() or 1
+    values, sample = [], ""
+    t0 = time.perf_counter()
+    for s in range(args.warmup + args.steps):
+        v, sample = cpu_job(g, descs, divisors, threads, args.cpu_target_s / max(1, args.steps))
+        if s >= args.warmup:
+            values.append(v)
+    wall = time.perf_counter() - t0
+    value = statistics.median(values) if values else 0.0
+    return {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "embeddings/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": wall * 1e3 / (args.warmup + args.steps),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32 ids / u64 counts",
+        "data": "synthetic (seeded R-MAT, no dataset)",
+        "config": {"workload": f"R-MAT scale {args.scale}, edge factor {EDGE_FACTOR}, seed {SEED}; six patterns with "
+                               "IEP, reference plans; whole-job throughput of the reference CPU path extrapolated "
+                               "from strided start-vertex slices"},
+        "cpu_baseline": {"value": value, "unit": "embeddings/s", "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": "embeddings/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    args = parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps(run_reference(args, world)), flush=True)
+        return
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=900))
+    line, g, plans, divisors = run_ours(args, world, rank, local)
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        v, sample = cpu_job(g, plan_descs(plans), divisors, os.cpu_count() or 1, args.cpu_target_s)
+        line["cpu_baseline"] = {"value": v, "unit": "embeddings/s", "cores": os.cpu_count() or 1, "kind": "port",
+                                "sample": sample}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

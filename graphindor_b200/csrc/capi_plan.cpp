@@ -90,6 +90,25 @@ static int build_dev_plan(const Schedule_IEP &s, DevPlan &d) {
         }
     }
     d.n_slots = slots;
+
+    // Lane-parallel leaf level: the candidates at depth stop - 1 are
+    // evaluated one per lane (sizes and counts only, no materialisation).
+    // Needs stop - 1 >= 2 and, for vertex-induced plans, no non-edge in the
+    // pattern (the per-candidate anti-edge filter stays warp-cooperative).
+    d.stop = d.iep_k > 0 ? n - d.iep_k : n - 1;
+    bool anti_edge = false;
+    for (int i = 0; i < n; ++i)
+        for (int j = 0; j < n; ++j)
+            if (i != j && !d.adj[i * n + j]) anti_edge = true;
+    d.leaf_depth = (d.stop - 1 >= 2 && !(d.vertex_induced && anti_edge)) ? d.stop - 1 : -1;
+    for (int p = 0; p < GI_MAX_PREFIX; ++p) d.pdepth[p] = p < tp ? s.get_prefix_data(p).back() : -1;
+    // Splitting of the depth-2 loop: its set's members are a subset of {0, 1}.
+    d.loop2_kind = -1;
+    if (d.stop > 2 && d.loop_set[2] >= 0) {
+        const auto &data = s.get_prefix_data(d.loop_set[2]);
+        if (data.size() == 1) d.loop2_kind = data[0];
+        else d.loop2_kind = 2;
+    }
     return GI_OK;
 }
 

@@ -75,6 +75,8 @@ void graph_free(gi_graph *g) {
     cudaFree(g->d_edge_from);
     cudaFree(g->d_scratch);
     cudaFree(g->d_counters);
+    cudaFree(g->d_offsets);
+    cudaFree(g->d_scan_tmp);
     cudaSetDevice(prev);
     delete g;
 }

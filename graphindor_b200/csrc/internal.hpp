@@ -31,6 +31,10 @@ struct DevPlan {
     int32_t n_slots;            // materialised prefixes = scratch slots per warp
     int32_t first_restricted;   // restrict_last[1] != -1: tasks need v1 < v0
     int32_t vertex_induced;
+    int32_t stop;               // depth closed in form: n - iep_k with IEP, else n - 1
+    int32_t leaf_depth;         // stop - 1 when its candidates run one per lane, else -1
+    int32_t loop2_kind;         // bound of the depth-2 loop set: 0 d(v0), 1 d(v1), 2 min, -1 none
+    int32_t pdepth[GI_MAX_PREFIX];  // last member (position) of each prefix
     int32_t father[GI_MAX_PREFIX];
     int32_t next[GI_MAX_PREFIX];
     int32_t break_size[GI_MAX_PREFIX];
@@ -78,6 +82,11 @@ struct gi_graph {
     void *d_scratch = nullptr;
     size_t scratch_bytes = 0;
     unsigned long long *d_counters = nullptr;  // [0] sum, [1] task cursor, [2] bytes, [3] tasks, ...
+    // Per-edge subtask offsets (exclusive scan) for splitting the depth-2
+    // loop, and the cub scan workspace; grown on demand.
+    int64_t *d_offsets = nullptr;
+    void *d_scan_tmp = nullptr;
+    size_t scan_tmp_bytes = 0;
     // Lazily built derived graphs (clique orientations).
     gi_graph *oriented[2] = {nullptr, nullptr};
 };

@@ -209,9 +209,33 @@ static void classify(const gi_plan_desc *P, int *size_only) {
 
 int oracle_count(const gi_plan_desc *P, const int64_t *vertex, const int32_t *edge, int32_t v_cnt,
                  int32_t v_begin, int32_t v_end, int threads, uint64_t *raw_sum, uint64_t *alg_bytes) {
-    if (!P || !vertex || !raw_sum || P->size < 3 || P->size > GI_MAX_PATTERN || v_cnt < 1) return -1;
+    return oracle_count_strided(P, vertex, edge, v_cnt, v_begin, v_end, 1, threads, raw_sum, alg_bytes);
+}
+
+static int count_core(const gi_plan_desc *P, const int64_t *vertex, const int32_t *edge, int32_t v_cnt,
+                      int32_t v_begin, int32_t v_end, int32_t stride, int threads, double max_seconds,
+                      uint64_t *raw_sum, uint64_t *alg_bytes, int64_t *processed);
+
+int oracle_count_strided(const gi_plan_desc *P, const int64_t *vertex, const int32_t *edge, int32_t v_cnt,
+                         int32_t v_begin, int32_t v_end, int32_t stride, int threads, uint64_t *raw_sum,
+                         uint64_t *alg_bytes) {
+    return count_core(P, vertex, edge, v_cnt, v_begin, v_end, stride, threads, 0.0, raw_sum, alg_bytes, NULL);
+}
+
+int oracle_count_timed(const gi_plan_desc *P, const int64_t *vertex, const int32_t *edge, int32_t v_cnt,
+                       int32_t stride, int threads, double max_seconds, uint64_t *raw_sum, int64_t *processed) {
+    return count_core(P, vertex, edge, v_cnt, 0, v_cnt, stride, threads, max_seconds, raw_sum, NULL, processed);
+}
+
+static int count_core(const gi_plan_desc *P, const int64_t *vertex, const int32_t *edge, int32_t v_cnt,
+                      int32_t v_begin, int32_t v_end, int32_t stride, int threads, double max_seconds,
+                      uint64_t *raw_sum, uint64_t *alg_bytes, int64_t *processed) {
+    if (!P || !vertex || !raw_sum || P->size < 3 || P->size > GI_MAX_PATTERN || v_cnt < 1 || stride < 1) return -1;
+    const double deadline = max_seconds > 0 ? omp_get_wtime() + max_seconds : 0.0;
+    int64_t done = 0;
     if (v_begin < 0) v_begin = 0;
     if (v_end > v_cnt) v_end = v_cnt;
+    const int64_t n_start = v_end > v_begin ? ((int64_t)v_end - v_begin + stride - 1) / stride : 0;
     int max_deg = 1;
     for (int32_t v = 0; v < v_cnt; ++v) {
         const int d = (int)(vertex[v + 1] - vertex[v]);
@@ -221,7 +245,7 @@ int oracle_count(const gi_plan_desc *P, const int64_t *vertex, const int32_t *ed
     int size_only[GI_MAX_PREFIX];
     classify(P, size_only);
     if (threads <= 0) threads = omp_get_max_threads();
-#pragma omp parallel num_threads(threads) reduction(+ : total, total_bytes)
+#pragma omp parallel num_threads(threads) reduction(+ : total, total_bytes, done)
     {
         dfs_t s;
         memset(&s, 0, sizeof(s));
@@ -236,10 +260,13 @@ int oracle_count(const gi_plan_desc *P, const int64_t *vertex, const int32_t *ed
         for (int p = 0; p < P->total_prefix_num; ++p) s.buf[p] = (int32_t *)malloc(sizeof(int32_t) * (size_t)max_deg);
         for (int d = 0; d <= GI_MAX_PATTERN; ++d) s.diff[d] = (int32_t *)malloc(sizeof(int32_t) * (size_t)max_deg);
 #pragma omp for schedule(dynamic, 16) nowait
-        for (int32_t v = v_begin; v < v_end; ++v) {
+        for (int64_t it = 0; it < n_start; ++it) {
+            if (deadline > 0 && omp_get_wtime() > deadline) continue;
+            const int32_t v = (int32_t)(v_begin + it * stride);
             for (int p = P->last[0]; p != -1; p = P->next[p]) build_vertex_set(&s, p, v);
             s.emb[0] = v;
             aggressive(&s, 1);
+            ++done;
         }
         total += s.sum;
         total_bytes += s.bytes;
@@ -248,6 +275,7 @@ int oracle_count(const gi_plan_desc *P, const int64_t *vertex, const int32_t *ed
     }
     *raw_sum = total;
     if (alg_bytes) *alg_bytes = total_bytes;
+    if (processed) *processed = done;
     return 0;
 }
 

@@ -32,6 +32,20 @@ extern "C" {
 int oracle_count(const gi_plan_desc *plan, const int64_t *vertex, const int32_t *edge, int32_t v_cnt,
                  int32_t v_begin, int32_t v_end, int threads, uint64_t *raw_sum, uint64_t *alg_bytes);
 
+/* The same over the start vertices v_begin, v_begin + stride, ... < v_end:
+ * an unbiased sample when vertex ids are randomly assigned (a contiguous id
+ * range is not: restrictions anchor each subgraph at one end of its id
+ * order).  Used for the timed CPU baseline. */
+int oracle_count_strided(const gi_plan_desc *plan, const int64_t *vertex, const int32_t *edge, int32_t v_cnt,
+                         int32_t v_begin, int32_t v_end, int32_t stride, int threads, uint64_t *raw_sum,
+                         uint64_t *alg_bytes);
+
+/* As oracle_count_strided, but no start vertex is begun once max_seconds
+ * have passed; *processed receives how many start vertices were counted
+ * (the sample is then those vertices). */
+int oracle_count_timed(const gi_plan_desc *plan, const int64_t *vertex, const int32_t *edge, int32_t v_cnt,
+                       int32_t stride, int threads, double max_seconds, uint64_t *raw_sum, int64_t *processed);
+
 /* Independent brute force: number of subgraphs of the graph isomorphic to
  * the n-vertex pattern adj (n*n '0'/'1'), edge-induced (induced = 0) or
  * vertex-induced (induced = 1), as #injective maps / #automorphisms.  For

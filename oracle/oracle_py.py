@@ -24,12 +24,17 @@ def build() -> Path:
 def lib():
     global _lib
     if _lib is None:
-        if not LIB.exists():
-            build()
+        build()  # incremental: rebuilds only when oracle.c changed
         L = C.CDLL(str(LIB))
         L.oracle_count.restype = C.c_int
         L.oracle_count.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_int,
                                    C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
+        L.oracle_count_strided.restype = C.c_int
+        L.oracle_count_strided.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_int32,
+                                           C.c_int32, C.c_int, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
+        L.oracle_count_timed.restype = C.c_int
+        L.oracle_count_timed.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_int,
+                                         C.c_double, C.POINTER(C.c_uint64), C.POINTER(C.c_int64)]
         L.oracle_brute_count.restype = C.c_uint64
         L.oracle_brute_count.argtypes = [C.c_int, C.c_char_p, C.c_int, C.c_void_p, C.c_void_p, C.c_int32]
         L.oracle_clique_count.restype = C.c_uint64
@@ -60,6 +65,31 @@ def count(plan_desc, vertex, edge, v_begin=0, v_end=None, threads=0, want_bytes=
     if rc != 0:
         raise ValueError("oracle_count rejected its input")
     return raw.value, (nb.value if want_bytes else None)
+
+
+def count_strided(plan_desc, vertex, edge, stride, v_begin=0, threads=0):
+    """Raw sum over the start vertices v_begin, v_begin + stride, ...: an
+    unbiased 1/stride sample when vertex ids are randomly assigned."""
+    vertex, edge = _arrays(vertex, edge)
+    n = len(vertex) - 1
+    raw = C.c_uint64()
+    rc = lib().oracle_count_strided(C.byref(plan_desc), vertex.ctypes.data, edge.ctypes.data, n, v_begin, n,
+                                    stride, threads, C.byref(raw), None)
+    if rc != 0:
+        raise ValueError("oracle_count_strided rejected its input")
+    return raw.value
+
+
+def count_timed(plan_desc, vertex, edge, stride, max_seconds, threads=0):
+    """(raw sum, start vertices counted) over every stride-th start vertex,
+    beginning no start vertex after max_seconds."""
+    vertex, edge = _arrays(vertex, edge)
+    raw, done = C.c_uint64(), C.c_int64()
+    rc = lib().oracle_count_timed(C.byref(plan_desc), vertex.ctypes.data, edge.ctypes.data, len(vertex) - 1,
+                                  stride, threads, max_seconds, C.byref(raw), C.byref(done))
+    if rc != 0:
+        raise ValueError("oracle_count_timed rejected its input")
+    return raw.value, done.value
 
 
 def brute(n, adj, vertex, edge, induced=False):
