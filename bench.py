@@ -7,15 +7,17 @@ diamond, 4-cycle, house, 5-clique, prism and 6-cycle with chord (0,3), each
 planned as the reference's gpu_graph plans them (analytic model, the
 reference's restriction generator, IEP on).
 
-The whole six-pattern job runs for hours, so the bench measures
-representative slices of it.  For pattern p, a slice is one shard of S_p:
-first-level subtasks are grouped in chunks and chunk c belongs to shard
-c mod S_p (the reference's static multi-device interleave), so every shard
-carries 1/S_p of the work, hubs included.  A step counts shard
-(step * world + rank) mod S_p of every pattern.
+The whole six-pattern job runs for days on any machine, so the bench
+measures random samples of it.  First-level work is cut into chunks of
+GI_TASK_CHUNK subtasks; a step counts, for every pattern, shard
+(step * world + rank) mod NSHARD of NSHARD with a device time budget: the
+shard's chunks are visited in a fixed pseudo-random order, no chunk starts
+after BUDGET_MS and chunks still running at 3 * BUDGET_MS are dropped, so
+the completed chunks (fraction f_p of the pattern's job) are a random
+sample of its work.
 
-value = whole-job throughput extrapolated from the slices:
-          sum_p (embeddings of p's shards) * S_p / sum_p (device time of p's shards) * S_p
+value = whole-job throughput estimated from the samples:
+          sum_p (embeddings counted for p) / f_p  over  sum_p (device time for p) / f_p
         with the graph resident in HBM (device time from CUDA events).
 e2e   = the same whole job through the public API from pinned host buffers:
         graph upload (H2D) + planning + counts + result reads (D2H).
@@ -51,8 +53,8 @@ PATTERNS = [
     ("prism", 6, "011100101010110001100011010101001110"),
     ("6-cycle+chord", 6, "010101101000010100101010000101100010"),
 ]
-SHARDS: dict = {}           # pattern -> S_p (calibrated unless given with --shards)
-TARGET_SHARD_MS = 1000.0     # device time of one calibrated shard
+NSHARD = 16                  # each step samples a different 1/16 of the chunks
+BUDGET_MS = 1000.0           # device time budget of one pattern's sample
 CPU_TARGET_S = 3.0           # host time of one pattern's CPU slice
 MEASURED = ROOT / "MEASURED_PEAKS.json"
 METRIC = "pattern-match embeddings/s, whole six-pattern job (R-MAT s22, IEP), 1 B200"
@@ -66,14 +68,9 @@ def parse_args():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--scale", type=int, default=SCALE)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--shards", default="", help="name=S,... fixes shard counts instead of calibrating")
-    ap.add_argument("--target-ms", type=float, default=TARGET_SHARD_MS)
+    ap.add_argument("--budget-ms", type=float, default=BUDGET_MS)
     ap.add_argument("--cpu-target-s", type=float, default=CPU_TARGET_S)
-    a = ap.parse_args()
-    for item in filter(None, a.shards.split(",")):
-        k, v = item.split("=")
-        SHARDS[k] = int(v)
-    return a
+    return ap.parse_args()
 
 
 def make_graph(scale: int):
@@ -131,28 +128,6 @@ class Clocks:
                 "samples": len(rows), "reasons": sorted(reasons)}
 
 
-def calibrate(L, N, graph, plans, sp, target_ms):
-    """Power-of-4 shard count per pattern whose shard 0 takes about target_ms."""
-    for name, _, _ in PATTERNS:
-        if name in SHARDS:
-            continue
-        S = 1 << 20
-        while True:
-            st = N.Stats()
-            st.budget_ms = 4.0 * target_ms
-            raw = C.c_uint64()
-            rc = L.gi_count_shard(graph.handle, plans[name].handle, 0, S, sp, C.byref(raw), C.byref(st))
-            if rc not in (N.GI_OK, N.GI_ETIMEOUT):
-                N.check(rc, "gi_count_shard")
-            if rc == N.GI_ETIMEOUT:
-                S = min(S * 4, 1 << 20)  # the previous, smaller shard
-                break
-            if st.kernel_ms >= target_ms / 4.0 or S == 1:
-                break
-            S //= 4
-        SHARDS[name] = max(1, S)
-
-
 def run_ours(args, world, rank, local):
     import torch
 
@@ -171,26 +146,29 @@ def run_ours(args, world, rank, local):
     dg = gi.Graph.from_csr(vertex_h, edge_h, tri_cnt=tri, stream=stream.cuda_stream)
     plans = {name: gi.Schedule_IEP(gi.Pattern(n, adj), dg.v_cnt, dg.e_cnt, tri) for name, n, adj in PATTERNS}
     divisors = {name: plans[name].export()["count_divisor"] for name, _, _ in PATTERNS}
-    calibrate(L, N, dg, plans, sp, args.target_ms)
-    if world > 1:
-        t = torch.tensor([SHARDS[name] for name, _, _ in PATTERNS], dtype=torch.int64, device="cuda")
-        torch.distributed.broadcast(t, 0)
-        for (name, _, _), s in zip(PATTERNS, t.tolist()):
-            SHARDS[name] = int(s)
 
     def one_step(graph, plan_map, step, acc, count_bytes=False):
         for name, _, _ in PATTERNS:
-            S = SHARDS[name]
             st = N.Stats()
             st.count_bytes = 1 if count_bytes else 0
+            st.budget_ms = args.budget_ms
+            st.allow_partial = 1
             raw = C.c_uint64()
-            N.check(L.gi_count_shard(graph.handle, plan_map[name].handle, (step * world + rank) % S, S, sp,
+            N.check(L.gi_count_shard(graph.handle, plan_map[name].handle, (step * world + rank) % NSHARD, NSHARD, sp,
                                      C.byref(raw), C.byref(st)), "gi_count_shard")
-            a = acc.setdefault(name, {"emb": 0.0, "ms": 0.0, "launches": 0, "bytes": 0})
+            f = st.chunks_done / max(1, st.chunks_total * NSHARD)  # fraction of the whole job
+            a = acc.setdefault(name, {"emb": 0.0, "ms": 0.0, "launches": 0, "bytes_per_chunk": 0.0, "chunks": 0,
+                                      "job_emb": 0.0, "job_ms": 0.0, "prep_ms": 0.0})
             a["emb"] += raw.value / divisors[name]
             a["ms"] += st.kernel_ms
+            a["prep_ms"] += st.prep_ms
             a["launches"] += st.kernel_launches
-            a["bytes"] += st.alg_bytes
+            a["chunks"] += st.chunks_done
+            if count_bytes and st.chunks_done:
+                a["bytes_per_chunk"] = st.alg_bytes / st.chunks_done
+            if f > 0:
+                a["job_emb"] += raw.value / divisors[name] / f
+                a["job_ms"] += st.prep_ms + st.kernel_ms / f
 
     def barrier():
         torch.cuda.synchronize()
@@ -237,35 +215,38 @@ def run_ours(args, world, rank, local):
         del g2, p2
     barrier()
 
-    # Reduce over ranks: device times take the max, work adds up.
+    # Whole-job estimates, averaged over the steps and summed over ranks
+    # (each rank samples its own shards; the job's time is the ranks' max).
     names = [n for n, _, _ in PATTERNS]
-    t_max = torch.tensor([dev_ms, e2e["upload_ms"], e2e["plan_ms"]] + [acc[n]["ms"] for n in names] +
-                         [e2e_acc[n]["ms"] for n in names], dtype=torch.float64, device="cuda")
-    w_sum = torch.tensor([acc[n]["emb"] for n in names] + [float(instr[n]["bytes"]) for n in names] +
-                         [float(acc[n]["launches"]) for n in names], dtype=torch.float64, device="cuda")
-    if world > 1:
-        torch.distributed.all_reduce(t_max, op=torch.distributed.ReduceOp.MAX)
-        torch.distributed.all_reduce(w_sum, op=torch.distributed.ReduceOp.SUM)
-    tm, ws = t_max.tolist(), w_sum.tolist()
     k = len(names)
-    dev_ms, up_ms, plan_ms = tm[0], tm[1], tm[2]
-    ms_p, e2e_ms_p = dict(zip(names, tm[3:3 + k])), dict(zip(names, tm[3 + k:3 + 2 * k]))
-    emb_p, bytes_p, launch_p = (dict(zip(names, ws[i * k:(i + 1) * k])) for i in range(3))
-
-    job_emb = sum(emb_p[n] * SHARDS[n] for n in names)
-    job_ms = sum(ms_p[n] * SHARDS[n] for n in names)
-    # e2e whole job: one upload and one planning per job, the counts scaled
-    # from their shards.
-    job_e2e_ms = up_ms / args.steps + plan_ms / args.steps + sum(e2e_ms_p[n] * SHARDS[n] for n in names)
+    vec = [acc[n]["job_emb"] for n in names] + [acc[n]["job_ms"] for n in names] + \
+          [e2e_acc[n]["job_ms"] for n in names] + [acc[n]["ms"] for n in names] + \
+          [instr[n]["bytes_per_chunk"] * acc[n]["chunks"] for n in names] + [float(acc[n]["launches"]) for n in names] + \
+          [dev_ms, e2e["upload_ms"], e2e["plan_ms"]]
+    t = torch.tensor(vec, dtype=torch.float64, device="cuda")
+    if world > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.SUM)
+        t /= world
+    v = t.tolist()
+    job_emb_p = dict(zip(names, v[0:k]))
+    job_ms_p = dict(zip(names, v[k:2 * k]))
+    e2e_job_ms_p = dict(zip(names, v[2 * k:3 * k]))
+    ms_p = dict(zip(names, v[3 * k:4 * k]))
+    bytes_p = dict(zip(names, v[4 * k:5 * k]))
+    launch_p = dict(zip(names, v[5 * k:6 * k]))
+    dev_ms, up_ms, plan_ms = v[6 * k:6 * k + 3]
+    job_emb = sum(job_emb_p.values()) / args.steps
+    job_ms = sum(job_ms_p.values()) / args.steps
+    job_e2e_ms = (up_ms + plan_ms + sum(e2e_job_ms_p.values())) / args.steps
 
     peaks = json.loads(MEASURED.read_text()) if MEASURED.exists() else {}
     hbm = float(peaks.get("hbm_gbs", 6650.0))
     total_bytes = sum(bytes_p.values())
     count_ms = sum(ms_p.values())
-    achieved = total_bytes / world / (count_ms / 1e3) / 1e9 if count_ms else 0.0
+    achieved = total_bytes / (count_ms / 1e3) / 1e9 if count_ms else 0.0
     line = {
         "metric": METRIC,
-        "value": job_emb / (job_ms / 1e3),
+        "value": job_emb * world / (job_ms / 1e3),
         "unit": "embeddings/s",
         "n_gpus": world,
         "steps": args.steps,
@@ -279,15 +260,15 @@ def run_ours(args, world, rank, local):
         "config": {
             "workload": f"R-MAT scale {args.scale}, edge factor {EDGE_FACTOR}, seed {SEED}: {g.v_cnt} vertices, "
                         f"{g.e_cnt // 2} undirected edges; six patterns with IEP, reference plans; whole-job "
-                        "throughput extrapolated from interleaved 1/S_p shards",
+                        f"throughput estimated from time-budgeted random samples ({args.budget_ms:.0f} ms per "
+                        f"pattern per step, 1/{NSHARD} shard per step)",
             "patterns": {n: adj for n, _, adj in PATTERNS},
-            "shards": dict(SHARDS),
-            "per_pattern_job_s": {n: ms_p[n] * SHARDS[n] / 1e3 / args.steps for n in names},
-            "per_pattern_embeddings": {n: emb_p[n] * SHARDS[n] / args.steps for n in names},
+            "per_pattern_job_s_estimate": {n: job_ms_p[n] / 1e3 / args.steps for n in names},
+            "per_pattern_embeddings_estimate": {n: job_emb_p[n] / args.steps for n in names},
             "l2": "inputs larger than L2 (CSR %.2f GB vs 126 MB)" % ((g.vertex.nbytes + g.edge.nbytes) / 1e9),
             "parallelism": f"dp{world}: shards interleaved across ranks",
         },
-        "e2e": {"value": job_emb / (job_e2e_ms / 1e3), "unit": "embeddings/s",
+        "e2e": {"value": job_emb * world / (job_e2e_ms / 1e3), "unit": "embeddings/s",
                 "h2d_bytes_per_step": int(g.vertex.nbytes + g.edge.nbytes),
                 "d2h_bytes_per_step": int(2 * 64 * len(PATTERNS)),
                 "upload_ms_per_step": up_ms / args.steps, "plan_ms_per_step": plan_ms / args.steps},
@@ -296,7 +277,7 @@ def run_ours(args, world, rank, local):
                      "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if MEASURED.exists() else "fallback",
                      "note": "achieved = algorithmic bytes of the counting launches (merge-intersection "
                              "accounting, counted by the instrumented kernel) / their CUDA-event time"},
-        "gpu_launches": int(sum(launch_p.values())),
+        "gpu_launches": int(round(sum(launch_p.values()) * world)),
         "clocks": clk,
     }
     return line, g, plans, divisors

@@ -71,7 +71,9 @@ class PlanDesc(C.Structure):
 class Stats(C.Structure):
     _fields_ = [("kernel_ms", C.c_double), ("raw_sum", C.c_uint64), ("tasks", C.c_uint64),
                 ("alg_bytes", C.c_uint64), ("count_bytes", C.c_int32), ("budget_ms", C.c_double),
-                ("grid_blocks", C.c_int32), ("block_threads", C.c_int32), ("kernel_launches", C.c_int32)]
+                ("grid_blocks", C.c_int32), ("block_threads", C.c_int32), ("kernel_launches", C.c_int32),
+                ("allow_partial", C.c_int32), ("chunks_done", C.c_int64), ("chunks_total", C.c_int64),
+                ("prep_ms", C.c_double)]
 
 
 # name -> (restype, argtypes)

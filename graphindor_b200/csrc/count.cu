@@ -48,7 +48,7 @@ constexpr int kTaskChunk = GI_TASK_CHUNK;
 constexpr unsigned kFull = 0xffffffffu;
 
 // Counter slots in gi_graph::d_counters.
-enum : int { kSum = 0, kCursor = 1, kBytes = 2, kTasks = 3, kTimeout = 4 };
+enum : int { kSum = 0, kCursor = 1, kBytes = 2, kTasks = 3, kTimeout = 4, kChunks = 5 };
 
 struct WarpState {
     const uint32_t *set_ptr[GI_MAX_PREFIX];
@@ -336,6 +336,20 @@ struct Ctx {
     WarpState &w;
     int lane;
     unsigned long long bytes;  // per lane in the leaf level, warp-uniform elsewhere (summed over lanes at the end / 1 lane)
+    unsigned long long t_start = 0;
+    unsigned long long hard_ns = 0;  // > 0: give up the current work item past this much time
+    bool aborted = false;
+
+    // Warp-uniform: true once the hard time limit has passed (lane 0's
+    // clock decides for the warp).
+    __device__ __forceinline__ bool out_of_time() {
+        if (!hard_ns) return false;
+        unsigned long long now = 0;
+        if (lane == 0) now = globaltimer();
+        now = __shfl_sync(kFull, now, 0);
+        if (now - t_start > hard_ns) aborted = true;
+        return aborted;
+    }
 
     // Builds every prefix whose last member is position d, with v placed at d.
     // Returns false when a prefix reaches its break size (no completion can
@@ -557,6 +571,7 @@ struct Ctx {
         __syncwarp();
         unsigned long long acc = 0;
         for (int base = i0; base < i1; base += 32) {
+            if (out_of_time()) break;
             const int i = base + lane;
             uint32_t v = 0;
             bool heavy = false;
@@ -599,6 +614,7 @@ struct Ctx {
         if (leaf == 2) return leaf_level(2, lo, hi);
         int d = 2;
         while (true) {
+            if (out_of_time()) break;
             if (d == stop) {
                 acc += P.iep_k > 0 ? iep_tail(d) : last_level(d);
                 --d;
@@ -676,20 +692,25 @@ __global__ void __launch_bounds__(kBlockThreads)
                      const uint32_t *__restrict__ edge, const uint32_t *__restrict__ edge_from, int64_t e_cnt,
                      const int64_t *__restrict__ offsets, int64_t n_tasks, int split, uint32_t *scratch,
                      int64_t slot_stride, unsigned long long *counters, unsigned long long budget_ns, int64_t shard,
-                     int64_t num_shards) {
+                     int64_t num_shards, int64_t n_chunks, int64_t perm_a, int64_t perm_b,
+                     unsigned long long hard_ns) {
     __shared__ WarpState states[kWarpsPerBlock];
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
     const int64_t gwarp = static_cast<int64_t>(blockIdx.x) * kWarpsPerBlock + wib;
     WarpState &w = states[wib];
     Ctx<kBytesOn> c{P, vertex, edge, scratch + gwarp * P.n_slots * slot_stride, slot_stride, w, lane, 0ull};
-    unsigned long long sum = 0, tasks = 0;
+    unsigned long long sum = 0, tasks = 0, chunks = 0;
     bool timed_out = false;
     const unsigned long long t_start = globaltimer();
+    c.t_start = t_start;
+    c.hard_ns = hard_ns;
     while (true) {
         // Claim the next chunk of kTaskChunk consecutive work items of this
-        // shard: chunk shard + j * num_shards (the reference's static
-        // interleave, gpu/src/gpu_pattern_matching_static_task.cuh:63).
+        // shard: slot shard + j * num_shards (the reference's static
+        // interleave, gpu/src/gpu_pattern_matching_static_task.cuh:63),
+        // mapped through the bijection slot -> (slot * perm_a + perm_b) mod
+        // n_chunks when a sampled count wants a pseudo-random order.
         unsigned long long j = 0;
         int stop = 0;
         if (lane == 0) {
@@ -701,8 +722,14 @@ __global__ void __launch_bounds__(kBlockThreads)
         }
         j = __shfl_sync(kFull, j, 0);
         stop = __shfl_sync(kFull, stop, 0);
-        const int64_t base = (shard + static_cast<int64_t>(j) * num_shards) * kTaskChunk;
-        if (stop || base >= n_tasks) break;
+        const int64_t slot = shard + static_cast<int64_t>(j) * num_shards;
+        if (stop || slot >= n_chunks) break;
+        const int64_t chunk = perm_a ? static_cast<int64_t>(
+                                           (static_cast<unsigned long long>(slot) * static_cast<unsigned long long>(perm_a) +
+                                            static_cast<unsigned long long>(perm_b)) %
+                                           static_cast<unsigned long long>(n_chunks))
+                                     : slot;
+        const int64_t base = chunk * kTaskChunk;
         const int64_t t = base + lane;
         bool valid = t < n_tasks;
         int64_t e = t;
@@ -730,6 +757,7 @@ __global__ void __launch_bounds__(kBlockThreads)
             if (!offsets && P.first_restricted && v0 <= v1) valid = false;
         }
         unsigned todo = __ballot_sync(kFull, valid);
+        unsigned long long chunk_sum = 0, chunk_tasks = 0;
         while (todo) {
             const int src = __ffs(todo) - 1;
             todo &= todo - 1;
@@ -751,14 +779,25 @@ __global__ void __launch_bounds__(kBlockThreads)
                 continue;
             }
             if (kBytesOn && !first) c.bytes = before;
-            tasks += first;
-            sum += c.dfs(sub_lo, offsets ? sub_lo + split : 0x7fffffff);
+            chunk_tasks += first;
+            chunk_sum += c.dfs(sub_lo, offsets ? sub_lo + split : 0x7fffffff);
+            if (c.aborted) break;
         }
+        // A chunk cut short by the hard limit is dropped whole, so the
+        // counted chunks stay a sample of complete work items.
+        if (c.aborted) {
+            timed_out = true;
+            break;
+        }
+        sum += chunk_sum;
+        tasks += chunk_tasks;
+        ++chunks;
     }
     const unsigned long long lane_bytes = kBytesOn ? warp_sum(c.bytes) : 0;
     if (lane == 0) {
         atomicAdd(&counters[kSum], sum);
         atomicAdd(&counters[kTasks], tasks);
+        atomicAdd(&counters[kChunks], chunks);
         if (kBytesOn) atomicAdd(&counters[kBytes], lane_bytes);
         if (timed_out) atomicExch(&counters[kTimeout], 1ull);
     }
@@ -846,8 +885,9 @@ int count_impl(gi_graph *g, const DevPlan &P, cudaStream_t st, uint64_t *raw_sum
     const size_t need = static_cast<size_t>(warps) * std::max(P.n_slots, 1) * stride * sizeof(uint32_t);
     int st_code = ensure_scratch(g, need);
     if (st_code != GI_OK) return st_code;
-    cudaEvent_t t0, t1;
+    cudaEvent_t t0, tm, t1;
     cudaEventCreate(&t0);
+    cudaEventCreate(&tm);
     cudaEventCreate(&t1);
     cudaEventRecord(t0, st);
     // Split the depth-2 loop when the plan has one; otherwise a work item is
@@ -860,6 +900,7 @@ int count_impl(gi_graph *g, const DevPlan &P, cudaStream_t st, uint64_t *raw_sum
         st_code = build_split(g, P, st, split, &n_tasks);
         if (st_code != GI_OK) {
             cudaEventDestroy(t0);
+            cudaEventDestroy(tm);
             cudaEventDestroy(t1);
             return st_code;
         }
@@ -869,32 +910,62 @@ int count_impl(gi_graph *g, const DevPlan &P, cudaStream_t st, uint64_t *raw_sum
         return cuda_fail(e, "counter reset");
     // Work budget: each warp stops claiming work once %globaltimer has
     // advanced budget_ns past its own start, and the call reports
-    // GI_ETIMEOUT.  No wait in the kernel depends on another warp.
+    // GI_ETIMEOUT.  No wait in the kernel depends on another warp.  A
+    // sampled count (allow_partial) visits the chunks in a pseudo-random
+    // order and drops chunks still running at three times the budget.
     const unsigned long long budget_ns = budget_ms > 0 ? static_cast<unsigned long long>(budget_ms * 1e6) : 0ull;
+    const bool partial = budget_ns && stats && stats->allow_partial;
     const int64_t *offs = use_split ? g->d_offsets : nullptr;
+    const int64_t n_chunks = (n_tasks + kTaskChunk - 1) / kTaskChunk;
+    int64_t perm_a = 0, perm_b = 0;
+    if (partial && n_chunks > 1) {
+        perm_a = static_cast<int64_t>(2654435761ull % static_cast<unsigned long long>(n_chunks));
+        auto gcd = [](int64_t x, int64_t y) {
+            while (y) {
+                const int64_t t = x % y;
+                x = y;
+                y = t;
+            }
+            return x;
+        };
+        if (perm_a == 0) perm_a = 1;
+        while (gcd(perm_a, n_chunks) != 1) perm_a = perm_a % (n_chunks - 1) + 1;
+        perm_b = n_chunks / 3;
+    }
+    const unsigned long long hard_ns = partial ? 3ull * budget_ns : 0ull;
+    cudaEventRecord(tm, st);
     if (bytes_on)
         dfs_count_kernel<true><<<blocks, kBlockThreads, 0, st>>>(
             P, g->d_vertex, reinterpret_cast<const uint32_t *>(g->d_edge), g->d_edge_from, g->e_cnt, offs, n_tasks,
-            split, static_cast<uint32_t *>(g->d_scratch), stride, g->d_counters, budget_ns, shard, num_shards);
+            split, static_cast<uint32_t *>(g->d_scratch), stride, g->d_counters, budget_ns, shard, num_shards, n_chunks,
+            perm_a, perm_b, hard_ns);
     else
         dfs_count_kernel<false><<<blocks, kBlockThreads, 0, st>>>(
             P, g->d_vertex, reinterpret_cast<const uint32_t *>(g->d_edge), g->d_edge_from, g->e_cnt, offs, n_tasks,
-            split, static_cast<uint32_t *>(g->d_scratch), stride, g->d_counters, budget_ns, shard, num_shards);
+            split, static_cast<uint32_t *>(g->d_scratch), stride, g->d_counters, budget_ns, shard, num_shards, n_chunks,
+            perm_a, perm_b, hard_ns);
     launches += 1;
     e = cudaGetLastError();
     cudaEventRecord(t1, st);
     unsigned long long host[8] = {0};
     if (e == cudaSuccess) e = cudaMemcpyAsync(host, g->d_counters, sizeof(host), cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-    float ms = 0.f;
-    if (e == cudaSuccess) cudaEventElapsedTime(&ms, t0, t1);
+    float ms = 0.f, prep = 0.f;
+    if (e == cudaSuccess) {
+        cudaEventElapsedTime(&prep, t0, tm);
+        cudaEventElapsedTime(&ms, tm, t1);
+    }
     cudaEventDestroy(t0);
+    cudaEventDestroy(tm);
     cudaEventDestroy(t1);
     if (e != cudaSuccess) return cuda_fail(e, "counting kernel");
-    if (host[kTimeout]) return fail(GI_ETIMEOUT, "count exceeded its device time budget");
+    if (host[kTimeout] && !partial) return fail(GI_ETIMEOUT, "count exceeded its device time budget");
     *raw_sum = host[kSum];
     if (stats) {
+        stats->chunks_done += static_cast<int64_t>(host[kChunks]);
+        stats->chunks_total += n_chunks > shard ? (n_chunks - shard + num_shards - 1) / num_shards : 0;
         stats->kernel_ms += ms;
+        stats->prep_ms += prep;
         stats->raw_sum = host[kSum];
         stats->tasks += host[kTasks];
         if (bytes_on) stats->alg_bytes += host[kBytes];
@@ -914,10 +985,12 @@ static void reset_stats(gi_stats *stats, double &budget) {
     budget = 0.0;
     if (!stats) return;
     const int cb = stats->count_bytes;
+    const int partial = stats->allow_partial;
     budget = stats->budget_ms;
     std::memset(stats, 0, sizeof(*stats));
     stats->count_bytes = cb;
     stats->budget_ms = budget;
+    stats->allow_partial = partial;
 }
 
 extern "C" int gi_count(const gi_graph *cg, const gi_plan *p, gi_stream stream, uint64_t *out_count,

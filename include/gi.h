@@ -190,6 +190,15 @@ typedef struct gi_stats {
     int32_t grid_blocks;     /* out: persistent blocks launched */
     int32_t block_threads;   /* out */
     int32_t kernel_launches; /* out: kernels of this library launched by the call */
+    int32_t allow_partial;   /* in (gi_count_shard only): with budget_ms > 0, return GI_OK and a
+                                partial raw_sum when the budget runs out.  Work items are then
+                                visited in a fixed pseudo-random order, no new item starts after
+                                budget_ms and items still running at 3 * budget_ms are dropped,
+                                so the completed items are a random sample of the shard */
+    int64_t chunks_done;     /* out: work chunks (GI_TASK_CHUNK subtasks each) counted */
+    int64_t chunks_total;    /* out: work chunks in the shard */
+    double prep_ms;          /* out: device time of the work-split pre-pass (once per count,
+                                not included in kernel_ms) */
 } gi_stats;
 
 /* Replaces gpu_pattern_matching<<<...>>> + the D2H of dev_sum + the

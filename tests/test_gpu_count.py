@@ -67,6 +67,40 @@ def test_validated_plans_are_exact(oracle):
                 assert gi.pattern_matching(dg, s).count == want, (n, adj, iep)
 
 
+def _shard(dg, s, shard, num, budget_ms=0.0, partial=False):
+    st = N.Stats()
+    st.budget_ms = budget_ms
+    st.allow_partial = 1 if partial else 0
+    raw = C.c_uint64()
+    N.check(gi.lib().gi_count_shard(dg.handle, s.handle, shard, num, None, C.byref(raw), C.byref(st)),
+            "gi_count_shard")
+    return raw.value, st
+
+
+@pytest.mark.parametrize("adj", ["0110100110010110", "011100101010110001100011010101001110"])
+def test_shards_add_up_to_the_whole_count(golden_graphs, dev_graphs, adj):
+    g, dg = golden_graphs["rmat_s10_ef12"], dev_graphs["rmat_s10_ef12"]
+    n = int(round(len(adj) ** 0.5))
+    s = gi.Schedule_IEP(gi.Pattern(n, adj), g.v_cnt, g.e_cnt, 0)
+    full = gi.pattern_matching(dg, s).raw_sum
+    for partial in (False, True):  # plain interleave, and the sampled (permuted) order with a roomy budget
+        total, done = 0, 0
+        for shard in range(5):
+            raw, st = _shard(dg, s, shard, 5, budget_ms=60000.0 if partial else 0.0, partial=partial)
+            assert st.chunks_done == st.chunks_total
+            total, done = (total + raw) % (1 << 64), done + st.chunks_done
+        assert total == full
+
+
+def test_time_budgeted_sample_returns_a_partial_count():
+    g = gen.rmat(14, 16.0, 9)
+    dg = gi.Graph.from_csr(g.vertex, g.edge)
+    s = gi.Schedule_IEP(gi.Pattern(6, "011100101010110001100011010101001110"), g.v_cnt, g.e_cnt, 0)
+    raw, st = _shard(dg, s, 0, 1, budget_ms=0.05, partial=True)
+    assert 0 <= st.chunks_done < st.chunks_total
+    assert st.prep_ms >= 0.0 and st.kernel_ms > 0.0
+
+
 def test_vertex_induced_plans(oracle):
     g = gen.erdos_renyi(60, 300, 5)
     dg = gi.Graph.from_csr(g.vertex, g.edge)
