@@ -222,6 +222,29 @@ int gi_count(const gi_graph *g, const gi_plan *p, gi_stream stream, uint64_t *ou
 int gi_count_shard(const gi_graph *g, const gi_plan *p, int32_t shard, int32_t num_shards, gi_stream stream,
                    uint64_t *raw_sum, gi_stats *stats);
 
+/* No counterpart in the reference.  The count of gi_count for callers that
+ * must not allocate device memory when they ask for it: code whose GPU
+ * memory is owned by another framework's pool, a serving loop that cannot
+ * afford cudaMalloc's latency and implicit synchronisation, a plug-in host
+ * that forbids allocations inside a request.  The caller passes the CSR it
+ * already holds on the current device (d_vertex[v_cnt+1] int64 offsets,
+ * d_edge[e_cnt] int32 sorted adjacency, as for gi_graph_create) and a device
+ * buffer d_result of two uint64: [0] the count, [1] the raw sum modulo 2^64.
+ * All working memory comes from one fixed device array of
+ * GI_NOALLOC_SCRATCH_BYTES that every GPU loading this code holds until the
+ * process exits; the call allocates nothing (no cudaMalloc, no cudaFree, no
+ * allocating library routine).  It launches as many warps as that array
+ * holds and returns GI_EOVERFLOW when even one block of four warps would
+ * need more (4 x materialised sets x second-largest degree x 4 bytes).  The
+ * first call on a device looks up the array's device address, so make that
+ * first call before any stream capture.  Calls share the array: two calls
+ * that overlap on the GPU (other streams, other threads) race and give wrong
+ * results.  Synchronous like gi_count; the CSR is checked on the device and
+ * a malformed one gives GI_EINVAL. */
+#define GI_NOALLOC_SCRATCH_BYTES (64u << 20)
+int gi_count_noalloc(const int64_t *d_vertex, const int32_t *d_edge, int32_t v_cnt, int64_t e_cnt,
+                     const gi_plan *p, gi_stream stream, uint64_t *d_result);
+
 /* Replaces gpu_clique (reference gpu/gpu_clique.cu:573-639) when
  * orientation = 0: k-cliques on the id-oriented DAG (keep u < v,
  * reference src/graph.cpp:710-735); and gpu_kclique (reference
