@@ -23,7 +23,7 @@ e2e   = the same whole job through the public API from pinned host buffers:
         graph upload (H2D) + planning + counts + result reads (D2H).
 cpu_baseline / --impl reference: the reference's CPU path (the oracle, a C
         restatement of reference src/graph.cpp:305-566) on all host cores
-        over every s_p-th start vertex (an unbiased slice: ids are random),
+        over every s_p-th directed edge (an unbiased slice: ids are random),
         extrapolated the same way.
 """
 from __future__ import annotations
@@ -302,22 +302,23 @@ def cpu_job(g, descs, divisors, threads, target_s):
     import oracle_py
     job_emb = job_s = 0.0
     parts = []
-    n = g.v_cnt
+    m = g.e_cnt
     for name, _, _ in PATTERNS:
-        stride = 1 << 20
+        stride = 1 << 22
         while True:
             t0 = time.perf_counter()
-            # A slice never runs much past 2 * target_s: no start vertex is
-            # begun after that; the extrapolation uses those counted.
-            raw, done = oracle_py.count_timed(descs[name], g.vertex, g.edge, stride, 2.0 * target_s, threads)
+            # Every stride-th directed edge (the reference's depth-1 loop
+            # entered per edge); no edge is begun after 2 * target_s and the
+            # extrapolation uses those counted.
+            raw, done = oracle_py.count_edges_timed(descs[name], g.vertex, g.edge, stride, 2.0 * target_s, threads)
             dt = time.perf_counter() - t0
             if dt >= target_s / 4.0 or stride == 1:
                 break
             stride //= 4
-        scale = n / max(1, done)
+        scale = m / max(1, done)
         job_emb += raw / divisors[name] * scale
         job_s += dt * scale
-        parts.append(f"{name}: {done} start vertices (every {stride}th), {dt:.2f}s")
+        parts.append(f"{name}: {done} edges (every {stride}th), {dt:.2f}s")
     return job_emb / job_s if job_s else 0.0, "; ".join(parts)
 
 

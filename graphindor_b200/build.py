@@ -99,7 +99,29 @@ def build(force: bool = False, verbose: bool = False) -> Path:
             sys.stderr.write(f"$ {' '.join(cmd)}\n{res.stdout}{res.stderr}\n")
         if res.returncode != 0:
             raise RuntimeError("link failed")
+    build_tools(force=force, verbose=verbose)
     return LIB
+
+
+TOOLS = {"gpu_graph": 1, "gpu_clique": 2, "gpu_kclique": 3, "gpu_mc": 4}
+BINDIR = PKG / "bin"
+
+
+def build_tools(force: bool = False, verbose: bool = False) -> None:
+    """The reference-compatible command-line tools, linked against the library."""
+    BINDIR.mkdir(exist_ok=True)
+    src = CSRC / "cli" / "gi_cli.cpp"
+    for name, tool in TOOLS.items():
+        out = BINDIR / name
+        if not force and out.exists() and out.stat().st_mtime >= max(src.stat().st_mtime, LIB.stat().st_mtime):
+            continue
+        cmd = [_host_cxx(), "-std=c++17", "-O2", f"-DGI_TOOL={tool}", f"-I{INCLUDE}", str(src), "-o", str(out),
+               f"-L{LIBDIR}", "-lgraphindor_b200", f"-Wl,-rpath,$ORIGIN/../lib"]
+        res = subprocess.run(cmd, capture_output=True, text=True)
+        if verbose or res.returncode != 0:
+            sys.stderr.write(f"$ {' '.join(cmd)}\n{res.stdout}{res.stderr}\n")
+        if res.returncode != 0:
+            raise RuntimeError(f"building {name} failed")
 
 
 def main() -> None:

@@ -279,6 +279,80 @@ static int count_core(const gi_plan_desc *P, const int64_t *vertex, const int32_
     return 0;
 }
 
+/* One iteration of the depth-1 loop of the reference CPU path (reference
+ * src/graph.cpp:537-565 at depth 1) for the candidate v1 of start vertex v0:
+ * restriction bound, injectivity, vertex-induced filter, the depth-1 prefix
+ * builds with the break-size prune, then the DFS from depth 2.  Summed over
+ * every directed edge (v0, v1) this is the whole count. */
+static void edge_task(dfs_t *s, int32_t v0, int32_t v1) {
+    const gi_plan_desc *P = s->P;
+    for (int p = P->last[0]; p != -1; p = P->next[p]) build_vertex_set(s, p, v0);
+    s->emb[0] = v0;
+    int32_t min_vertex = s->v_cnt;
+    for (int i = P->restrict_last[1]; i != -1; i = P->restrict_next[i])
+        if (min_vertex > s->emb[P->restrict_index[i]]) min_vertex = s->emb[P->restrict_index[i]];
+    if (min_vertex <= v1 || v1 == v0) return;
+    if (P->is_vertex_induced) {
+        int32_t out;
+        if (remove_anti_edge(s, &v1, 1, &out, 1) == 0) return;
+    }
+    for (int p = P->last[1]; p != -1; p = P->next[p]) {
+        build_vertex_set(s, p, v1);
+        if (s->size[p] == P->break_size[p]) return;
+    }
+    s->emb[1] = v1;
+    aggressive(s, 2);
+}
+
+int oracle_count_edges_timed(const gi_plan_desc *P, const int64_t *vertex, const int32_t *edge, int32_t v_cnt,
+                             int64_t stride, int threads, double max_seconds, uint64_t *raw_sum, int64_t *processed) {
+    if (!P || !vertex || !raw_sum || P->size < 3 || P->size > GI_MAX_PATTERN || v_cnt < 1 || stride < 1) return -1;
+    const int64_t e_cnt = vertex[v_cnt];
+    const int64_t n_edges = (e_cnt + stride - 1) / stride;
+    const double deadline = max_seconds > 0 ? omp_get_wtime() + max_seconds : 0.0;
+    int max_deg = 1;
+    for (int32_t v = 0; v < v_cnt; ++v) {
+        const int d = (int)(vertex[v + 1] - vertex[v]);
+        if (d > max_deg) max_deg = d;
+    }
+    uint64_t total = 0;
+    int64_t done = 0;
+    if (threads <= 0) threads = omp_get_max_threads();
+#pragma omp parallel num_threads(threads) reduction(+ : total, done)
+    {
+        dfs_t s;
+        memset(&s, 0, sizeof(s));
+        s.P = P;
+        s.vertex = vertex;
+        s.edge = edge;
+        s.v_cnt = v_cnt;
+        s.n = P->size;
+        s.k = P->in_exclusion_optimize_num;
+        for (int p = 0; p < P->total_prefix_num; ++p) s.buf[p] = (int32_t *)malloc(sizeof(int32_t) * (size_t)max_deg);
+        for (int d = 0; d <= GI_MAX_PATTERN; ++d) s.diff[d] = (int32_t *)malloc(sizeof(int32_t) * (size_t)max_deg);
+#pragma omp for schedule(dynamic, 64) nowait
+        for (int64_t it = 0; it < n_edges; ++it) {
+            if (deadline > 0 && omp_get_wtime() > deadline) continue;
+            const int64_t e = it * stride;
+            /* source vertex: the last v with vertex[v] <= e */
+            int32_t lo = 0, hi = v_cnt;
+            while (hi - lo > 1) {
+                const int32_t mid = lo + (hi - lo) / 2;
+                if (vertex[mid] <= e) lo = mid;
+                else hi = mid;
+            }
+            edge_task(&s, lo, edge[e]);
+            ++done;
+        }
+        total += s.sum;
+        for (int p = 0; p < P->total_prefix_num; ++p) free(s.buf[p]);
+        for (int d = 0; d <= GI_MAX_PATTERN; ++d) free(s.diff[d]);
+    }
+    *raw_sum = total;
+    if (processed) *processed = done;
+    return 0;
+}
+
 /* ------------------------------------------------------------ brute force */
 
 static int adjacent(const int64_t *vertex, const int32_t *edge, int32_t a, int32_t b) {

@@ -152,6 +152,32 @@ def test_budget_expiry_returns_timeout_and_device_stays_usable():
     assert gi.pattern_matching(dg, s3).count == gi.clique_count(dg, 3, 1).count
 
 
+def test_cli_tools_print_the_reference_lines(tmp_path, golden_counts, golden_graphs):
+    """gpu_graph / gpu_clique / gpu_kclique / gpu_mc with the reference's argv
+    print the reference's result lines with the reference's counts."""
+    import re
+    import subprocess
+    from pathlib import Path
+    bindir = Path(gi.__file__).resolve().parent / "bin"
+    name = "rmat_s9_ef8"
+    g = golden_graphs[name]
+    path = tmp_path / "g.g"
+    gi.write_g(str(path), g.vertex, g.edge, g.max_intersection_size, 0)
+    adj = "0101110101010101010011000"
+    out = subprocess.run([str(bindir / "gpu_graph"), str(path), "5", adj], capture_output=True, text=True,
+                         check=True).stdout
+    assert int(re.search(r"Pattern count: (\d+)", out).group(1)) == golden_counts["patterns"][name][adj]
+    assert re.search(r"Counting time cost: [\d.]+ s", out)
+    out = subprocess.run([str(bindir / "gpu_clique"), str(path), "4"], capture_output=True, text=True,
+                         check=True).stdout
+    assert int(re.search(r"count (\d+)", out).group(1)) == golden_counts["cliques"][name]["4"]
+    out = subprocess.run([str(bindir / "gpu_kclique"), str(path), "5"], capture_output=True, text=True,
+                         check=True).stdout
+    assert int(re.search(r"Answer: (\d+)", out).group(1)) == golden_counts["cliques"][name]["5"]
+    out = subprocess.run([str(bindir / "gpu_mc"), str(path), "4"], capture_output=True, text=True, check=True).stdout
+    assert [int(x) for x in re.findall(r"Pattern count: (\d+)", out)] == golden_counts["motifs"][name]["4"]
+
+
 def test_rejects_malformed_graphs(native):
     vertex = np.array([0, 2, 3, 4], dtype=np.int64)
     edge = np.array([2, 1, 0, 0], dtype=np.int32)  # unsorted list of vertex 0

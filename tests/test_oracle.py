@@ -92,6 +92,23 @@ def test_validated_plans_match_brute_force(oracle, native):
                 assert got == want, (n, adj, iep)
 
 
+def test_edge_sampled_counts_partition_the_whole(oracle, golden_graphs):
+    """Counting per directed edge (the CPU baseline's sampling unit) sums to
+    the per-start-vertex count, and the strided slices partition it."""
+    g = golden_graphs["rmat_s10_ef12"]
+    for n, adj in [(4, "0110100110010110"), (5, "0101110101010101010011000"),
+                   (6, "011100101010110001100011010101001110")]:
+        s = gi.Schedule_IEP(gi.Pattern(n, adj), g.v_cnt, g.e_cnt, 0)
+        d = plan_desc(s)
+        whole, _ = oracle.count(d, g.vertex, g.edge, threads=4)
+        raw, done = oracle.count_edges_timed(d, g.vertex, g.edge, 1, threads=4)
+        assert raw == whole and done == g.e_cnt
+    s = gi.Schedule_IEP(gi.Pattern(3, "011101110"), vertex_induced=True)
+    d = plan_desc(s)
+    whole, _ = oracle.count(d, g.vertex, g.edge, threads=4)
+    assert oracle.count_edges_timed(d, g.vertex, g.edge, 1, threads=4)[0] == whole
+
+
 def test_oracle_cliques_and_triangles(oracle, golden_counts, golden_graphs):
     for name, cl in golden_counts["cliques"].items():
         g = golden_graphs[name]
