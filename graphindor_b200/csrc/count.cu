@@ -62,8 +62,13 @@ __global__ void split_count_kernel(const __grid_constant__ DevPlan P, const int6
     }
 }
 
-template <bool kBytesOn>
-__global__ void __launch_bounds__(kBlockThreads)
+// kMinBlocks: resident blocks per SM the register allocation is held to.
+// Deep plans (six or more pattern vertices) spend their time in long chains
+// of dependent loads and gain from the extra resident warps despite some
+// spilling (R-MAT scale 22: prism 1.6x, 6-cycle+chord 1.6x faster at 16
+// blocks); shallower plans run best with the unconstrained allocation.
+template <bool kBytesOn, int kMinBlocks>
+__global__ void __launch_bounds__(kBlockThreads, kMinBlocks)
     dfs_count_kernel(const __grid_constant__ DevPlan P, const int64_t *__restrict__ vertex,
                      const uint32_t *__restrict__ edge, const uint32_t *__restrict__ edge_from, int64_t e_cnt,
                      const int64_t *__restrict__ offsets, int64_t n_tasks, int split, uint32_t *scratch,
@@ -239,6 +244,16 @@ static int build_split(gi_graph *g, const DevPlan &P, cudaStream_t st, int split
     return GI_OK;
 }
 
+using DfsKernel = decltype(&dfs_count_kernel<false, 1>);
+
+// The instantiation for a plan: byte counting on or off, and the occupancy
+// target by pattern size.
+DfsKernel pick_dfs_kernel(bool bytes_on, int n) {
+    const bool deep = n >= 6;
+    if (bytes_on) return deep ? dfs_count_kernel<true, 16> : dfs_count_kernel<true, 1>;
+    return deep ? dfs_count_kernel<false, 16> : dfs_count_kernel<false, 1>;
+}
+
 // Runs the counting kernel for one plan on one graph (or one shard of it).
 // budget_ms = 0 means no budget.
 int count_impl(gi_graph *g, const DevPlan &P, cudaStream_t st, uint64_t *raw_sum, gi_stats *stats,
@@ -250,10 +265,8 @@ int count_impl(gi_graph *g, const DevPlan &P, cudaStream_t st, uint64_t *raw_sum
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, g->device);
     const bool bytes_on = stats && stats->count_bytes;
     cudaError_t e;
-    if (bytes_on)
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, dfs_count_kernel<true>, kBlockThreads, 0);
-    else
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, dfs_count_kernel<false>, kBlockThreads, 0);
+    const auto kernel = pick_dfs_kernel(bytes_on, P.n);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, kernel, kBlockThreads, 0);
     if (e != cudaSuccess) return cuda_fail(e, "occupancy query");
     const int blocks = sms * std::max(1, blocks_per_sm);
     const int64_t warps = static_cast<int64_t>(blocks) * kWarpsPerBlock;
@@ -310,16 +323,10 @@ int count_impl(gi_graph *g, const DevPlan &P, cudaStream_t st, uint64_t *raw_sum
     }
     const unsigned long long hard_ns = partial ? 3ull * budget_ns : 0ull;
     cudaEventRecord(tm, st);
-    if (bytes_on)
-        dfs_count_kernel<true><<<blocks, kBlockThreads, 0, st>>>(
-            P, g->d_vertex, reinterpret_cast<const uint32_t *>(g->d_edge), g->d_edge_from, g->e_cnt, offs, n_tasks,
-            split, static_cast<uint32_t *>(g->d_scratch), stride, g->d_counters, budget_ns, shard, num_shards, n_chunks,
-            perm_a, perm_b, hard_ns);
-    else
-        dfs_count_kernel<false><<<blocks, kBlockThreads, 0, st>>>(
-            P, g->d_vertex, reinterpret_cast<const uint32_t *>(g->d_edge), g->d_edge_from, g->e_cnt, offs, n_tasks,
-            split, static_cast<uint32_t *>(g->d_scratch), stride, g->d_counters, budget_ns, shard, num_shards, n_chunks,
-            perm_a, perm_b, hard_ns);
+    kernel<<<blocks, kBlockThreads, 0, st>>>(P, g->d_vertex, reinterpret_cast<const uint32_t *>(g->d_edge),
+                                             g->d_edge_from, g->e_cnt, offs, n_tasks, split,
+                                             static_cast<uint32_t *>(g->d_scratch), stride, g->d_counters, budget_ns,
+                                             shard, num_shards, n_chunks, perm_a, perm_b, hard_ns);
     launches += 1;
     e = cudaGetLastError();
     cudaEventRecord(t1, st);
