@@ -17,7 +17,8 @@ from . import _native as N
 from ._native import GIError, check, lib
 
 __all__ = ["Pattern", "Schedule_IEP", "Graph", "pattern_matching", "clique_count", "motif_counting",
-           "motif_patterns", "GIError", "lib", "write_g", "read_g"]
+           "motif_patterns", "GIError", "lib", "write_g", "read_g", "LabeledGraph", "fsm", "fsm_plan",
+           "FsmResult", "PATENTS_TRI_CNT", "YOUTUBE_TRI_CNT"]
 
 
 class Pattern:
@@ -277,3 +278,113 @@ def read_g(path: str):
     edge = np.empty(max(1, e.value), dtype=np.int32)
     check(L.gi_g_read(str(path).encode(), vertex.ctypes.data, edge.ctypes.data, v.value, e.value), "gi_g_read")
     return vertex, edge[: e.value], int(mi.value), int(tri.value)
+
+
+# ------------------------------------------------------------ labeled graphs + FSM
+
+PATENTS_TRI_CNT = 7515023      # the constant fsm_test plans with (reference include/dataloader.h:28)
+YOUTUBE_TRI_CNT = 103017122    # the constant gpu_fsm plans with (reference include/dataloader.h:35)
+
+
+class LabeledGraph:
+    """Labeled graph in the reference loader's numbering (reference
+    include/labeled_graph.h, src/dataloader.cpp:381-625): labels renamed by
+    descending maximum degree, vertices sorted by (label, -degree, id), each
+    neighbour list bucketed by neighbour label.  Built on the host; copied to
+    the current device by the first :func:`fsm`."""
+
+    def __init__(self, handle: C.c_void_p):
+        self._h = handle
+        info = N.LabeledGraphInfo()
+        check(lib().gi_labeled_graph_get_info(handle, C.byref(info)), "gi_labeled_graph_get_info")
+        self.v_cnt, self.e_cnt, self.l_cnt = info.v_cnt, info.e_cnt, info.l_cnt
+
+    @classmethod
+    def from_csr(cls, vertex: np.ndarray, edge: np.ndarray, labels: np.ndarray,
+                 order: Optional[np.ndarray] = None) -> "LabeledGraph":
+        """``vertex``/``edge``: symmetric CSR in original ids; ``labels``:
+        original label value per vertex; ``order``: the order of the vertex
+        lines (default ascending id)."""
+        vertex = np.ascontiguousarray(vertex, dtype=np.int64)
+        edge = np.ascontiguousarray(edge, dtype=np.int32)
+        labels = np.ascontiguousarray(labels, dtype=np.uint32)
+        if order is not None:
+            order = np.ascontiguousarray(order, dtype=np.int32)
+        h = C.c_void_p()
+        check(lib().gi_labeled_graph_create(len(vertex) - 1, vertex.ctypes.data,
+                                            edge.ctypes.data if edge.size else None, labels.ctypes.data,
+                                            order.ctypes.data if order is not None else None, C.byref(h)),
+              "gi_labeled_graph_create")
+        return cls(h)
+
+    @classmethod
+    def load_adj(cls, path: str) -> "LabeledGraph":
+        h = C.c_void_p()
+        check(lib().gi_labeled_graph_load_adj(str(path).encode(), C.byref(h)), "gi_labeled_graph_load_adj")
+        return cls(h)
+
+    def export(self) -> dict:
+        """Host copies of the renumbered structure."""
+        v, l, e = self.v_cnt, self.l_cnt, self.e_cnt
+        out = {"new_id": np.empty(v, np.int32), "v_label": np.empty(v, np.int32),
+               "label_value": np.empty(l, np.uint32), "label_start": np.empty(l + 1, np.uint32),
+               "bucket": np.empty(v * l + 1, np.uint32), "edge": np.empty(max(e, 1), np.uint32)}
+        check(lib().gi_labeled_graph_export(self._h, *[out[k].ctypes.data for k in
+                                                       ("new_id", "v_label", "label_value", "label_start",
+                                                        "bucket", "edge")]), "gi_labeled_graph_export")
+        out["edge"] = out["edge"][:e]
+        return out
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            lib().gi_labeled_graph_destroy(h)
+            self._h = None
+
+    @property
+    def handle(self) -> C.c_void_p:
+        return self._h
+
+
+def _fsm_pattern(p: N.FsmPattern) -> dict:
+    n = p.n
+    return {"n": n, "edges": p.edges, "adj": p.adj[: n * n].decode(),
+            "restricts": [(p.restricts[i][0], p.restricts[i][1]) for i in range(p.n_restricts)],
+            "automorphisms": p.n_automorphisms, "jobs": p.jobs, "frequent": p.frequent, "kernel_ms": p.kernel_ms}
+
+
+@dataclass
+class FsmResult:
+    count: int
+    kernel_ms: float
+    total_ms: float
+    jobs: int
+    candidates: int
+    kernel_launches: int
+    patterns: list
+
+
+def fsm(graph: LabeledGraph, max_edge: int, min_support: int, tri_cnt: int = YOUTUBE_TRI_CNT, *,
+        stream: int = 0) -> FsmResult:
+    """Number of frequent labeled patterns with exactly ``max_edge`` edges
+    under MNI support (gpu_fsm / LabeledGraph::fsm semantics).  ``tri_cnt``
+    is the triangle count the planner is given (gpu_fsm uses YouTube's
+    constant, fsm_test Patents')."""
+    pats = (N.FsmPattern * N.GI_FSM_MAX_PATTERNS)()
+    st = N.FsmStats()
+    st.patterns = C.cast(pats, C.POINTER(N.FsmPattern))
+    out = C.c_int64()
+    check(lib().gi_fsm(graph.handle, max_edge, int(min_support), int(tri_cnt), C.c_void_p(stream) if stream else None,
+                       C.byref(out), C.byref(st)), "gi_fsm")
+    return FsmResult(out.value, st.kernel_ms, st.total_ms, st.jobs, st.candidates, st.kernel_launches,
+                     [_fsm_pattern(pats[i]) for i in range(st.n_patterns)])
+
+
+def fsm_plan(max_edge: int, v_cnt: int, e_cnt: int, tri_cnt: int = YOUTUBE_TRI_CNT) -> list[dict]:
+    """The unlabeled patterns of an FSM run with their plans (schedule-order
+    adjacency, label restrictions (d, r): label[d] <= label[r])."""
+    pats = (N.FsmPattern * N.GI_FSM_MAX_PATTERNS)()
+    cnt = C.c_int()
+    check(lib().gi_fsm_plan(max_edge, v_cnt, e_cnt, tri_cnt, pats, N.GI_FSM_MAX_PATTERNS, C.byref(cnt)),
+          "gi_fsm_plan")
+    return [_fsm_pattern(pats[i]) for i in range(min(cnt.value, N.GI_FSM_MAX_PATTERNS))]

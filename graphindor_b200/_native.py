@@ -76,6 +76,25 @@ class Stats(C.Structure):
                 ("prep_ms", C.c_double)]
 
 
+class LabeledGraphInfo(C.Structure):
+    _fields_ = [("v_cnt", C.c_int32), ("e_cnt", C.c_int64), ("l_cnt", C.c_int32), ("device", C.c_int32)]
+
+
+GI_FSM_MAX_PATTERNS = 64
+
+
+class FsmPattern(C.Structure):
+    _fields_ = [("n", C.c_int32), ("edges", C.c_int32), ("adj", C.c_char * (GI_MAX_PATTERN * GI_MAX_PATTERN)),
+                ("n_restricts", C.c_int32), ("restricts", (C.c_int32 * 2) * 21), ("n_automorphisms", C.c_int32),
+                ("jobs", C.c_int64), ("frequent", C.c_int64), ("kernel_ms", C.c_double)]
+
+
+class FsmStats(C.Structure):
+    _fields_ = [("kernel_ms", C.c_double), ("total_ms", C.c_double), ("jobs", C.c_int64),
+                ("candidates", C.c_int64), ("kernel_launches", C.c_int32), ("n_patterns", C.c_int32),
+                ("patterns", C.POINTER(FsmPattern))]
+
+
 # name -> (restype, argtypes)
 _SIGS = {
     "gi_status_string": (C.c_char_p, [C.c_int]),
@@ -109,6 +128,16 @@ _SIGS = {
     "gi_motif_num": (C.c_int, [C.c_int]),
     "gi_motif_patterns": (C.c_int, [C.c_int, C.c_char_p, C.c_int]),
     "gi_motif_count": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.POINTER(Stats)]),
+    "gi_labeled_graph_create": (C.c_int, [C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                          C.POINTER(C.c_void_p)]),
+    "gi_labeled_graph_load_adj": (C.c_int, [C.c_char_p, C.POINTER(C.c_void_p)]),
+    "gi_labeled_graph_destroy": (C.c_int, [C.c_void_p]),
+    "gi_labeled_graph_get_info": (C.c_int, [C.c_void_p, C.POINTER(LabeledGraphInfo)]),
+    "gi_labeled_graph_export": (C.c_int, [C.c_void_p] + [C.c_void_p] * 6),
+    "gi_fsm": (C.c_int, [C.c_void_p, C.c_int, C.c_int64, C.c_int64, C.c_void_p, C.POINTER(C.c_int64),
+                         C.POINTER(FsmStats)]),
+    "gi_fsm_plan": (C.c_int, [C.c_int, C.c_int32, C.c_int64, C.c_int64, C.POINTER(FsmPattern), C.c_int,
+                              C.POINTER(C.c_int)]),
 }
 
 _lib = None

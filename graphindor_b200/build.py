@@ -103,7 +103,7 @@ def build(force: bool = False, verbose: bool = False) -> Path:
     return LIB
 
 
-TOOLS = {"gpu_graph": 1, "gpu_clique": 2, "gpu_kclique": 3, "gpu_mc": 4}
+TOOLS = {"gpu_graph": 1, "gpu_clique": 2, "gpu_kclique": 3, "gpu_mc": 4, "gpu_fsm": 5}
 BINDIR = PKG / "bin"
 
 

@@ -359,7 +359,9 @@ int gi_plan_candidates(int n, const char *adj, int32_t v_cnt, int64_t e_cnt, int
 // (reference src/motif_generator.cpp:5-43): edges (i,j), i<j, taken in
 // row-major order with "use the edge" explored before "skip it"; a pattern is
 // emitted when it is connected and no relabelling of it was emitted before.
-static std::vector<std::vector<int>> motif_list(int k) {
+}  // extern "C"
+
+std::vector<std::vector<int>> gi::motif_list(int k) {
     std::vector<std::vector<int>> out;
     std::set<std::set<int>> seen;
     std::vector<std::pair<int, int>> edges;
@@ -402,6 +404,8 @@ static std::vector<std::vector<int>> motif_list(int k) {
     rec(0);
     return out;
 }
+
+extern "C" {
 
 int gi_motif_num(int k) {
     if (k < 3 || k > GI_MAX_PATTERN) return -1;

@@ -5,9 +5,10 @@
 //   2 gpu_clique  <graph.g> <clique_size>                             (reference gpu/gpu_clique.cu:573-639)
 //   3 gpu_kclique <graph.g> <clique_size>                             (reference gpu/gpu_kclique.cu:517-546)
 //   4 gpu_mc      <graph.g> <motif_size>                              (reference gpu/gpu_mc.cu:62-119)
+//   5 gpu_fsm     <graph.adj> <max_edge> <min_support>                (reference gpu/gpu_fsm.cu:926-950)
 // Each prints the same result line as the reference tool ("Pattern count:",
-// "count", "Answer:", one "Pattern count:" per motif) and "Counting time
-// cost: X s".  Failures go to stderr with the status text; no tool calls
+// "count", "Answer:", one "Pattern count:" per motif, "fsm cnt =") and
+// "Counting time cost: X s".  Failures go to stderr with the status text; no tool calls
 // exit() from inside the library.
 #include <sys/time.h>
 
@@ -136,6 +137,29 @@ int main(int argc, char **argv) {
     else
         std::printf("Answer: %llu\n", static_cast<unsigned long long>(count));
     std::printf("Counting time cost: %.6lf s.\n", dt);
+    return 0;
+#elif GI_TOOL == 5
+    if (argc < 4) {
+        std::fprintf(stderr, "Usage: %s graph.adj max_edge min_support\n", argv[0]);
+        return 1;
+    }
+    gi_labeled_graph *g = nullptr;
+    const double t_load = now_s();
+    int st = gi_labeled_graph_load_adj(argv[1], &g);
+    if (st != GI_OK) return report(st, "data load failure");
+    std::fprintf(stderr, "Load data success! time: %g seconds\n", now_s() - t_load);
+    const int max_edge = std::atoi(argv[2]);
+    const long long min_support = std::atoll(argv[3]);
+    // gpu_fsm plans with the YouTube triangle count (reference gpu/gpu_fsm.cu:939).
+    const double t0 = now_s();
+    int64_t cnt = 0;
+    st = gi_fsm(g, max_edge, min_support, 103017122LL, nullptr, &cnt, nullptr);
+    const double dt = now_s() - t0;
+    gi_labeled_graph_destroy(g);
+    if (st != GI_OK) return report(st, "fsm failed");
+    std::printf("Counting time cost: %ld.%06ld s.\n", static_cast<long>(dt),
+                static_cast<long>((dt - static_cast<long>(dt)) * 1e6));
+    std::printf("fsm cnt = %lld\n", static_cast<long long>(cnt));
     return 0;
 #else
     if (argc < 3) {

@@ -15,6 +15,10 @@ namespace gi {
 // Records a failure message for gi_last_error() and returns the status.
 int fail(int status, const std::string &msg);
 
+// Connected k-vertex patterns (row-major k*k 0/1 matrices) in the order of
+// the reference MotifGenerator; k >= 2.
+std::vector<std::vector<int>> motif_list(int k);
+
 // Per-prefix build mode used by the counting kernels.
 enum PrefixMode : int32_t {
     kAlias = 0,        // father == -1: the set is N(v) itself, no copy

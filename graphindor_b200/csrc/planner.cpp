@@ -261,7 +261,7 @@ Schedule_IEP::Schedule_IEP(const Pattern &pattern, bool &is_pattern_valid, int p
                            int restricts_type, bool use_in_exclusion_optimize, int v_cnt, int64_t e_cnt,
                            long long tri_cnt, bool vertex_induced) {
     const int n = pattern.get_size();
-    if (n < 3 || n > kMaxPatternSize)
+    if (n < 2 || n > kMaxPatternSize)
         throw std::invalid_argument("pattern size must be between 3 and 7");
     if (performance_modeling_type < 0 || performance_modeling_type > 1)
         throw std::invalid_argument("only performance_modeling_type 0 and 1 are supported");
@@ -359,7 +359,7 @@ Schedule_IEP::Schedule_IEP(const Pattern &pattern, bool &is_pattern_valid, int p
 Schedule_IEP::Schedule_IEP(const Pattern &pattern, const std::vector<int> &order, const Pairs &restricts,
                            bool use_in_exclusion_optimize, bool exact) {
     const int n = pattern.get_size();
-    if (n < 3 || n > kMaxPatternSize)
+    if (n < 2 || n > kMaxPatternSize)
         throw std::invalid_argument("pattern size must be between 3 and 7");
     if (static_cast<int>(order.size()) != n)
         throw std::invalid_argument("order must list every pattern vertex once");
@@ -954,7 +954,7 @@ std::vector<Schedule_IEP::Candidate> Schedule_IEP::enumerate_candidates(const Pa
                                                                        long long tri_cnt) {
     std::vector<Candidate> out;
     const int n = pattern.get_size();
-    if (n < 3 || n > kMaxPatternSize || !pattern.check_connected()) return out;
+    if (n < 2 || n > kMaxPatternSize || !pattern.check_connected()) return out;
     Schedule_IEP s;
     s.alloc(n);
     std::copy(pattern.get_adj_mat_ptr(), pattern.get_adj_mat_ptr() + n * n, s.adj_mat.begin());

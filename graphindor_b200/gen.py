@@ -90,3 +90,44 @@ def from_edges(n: int, edges) -> CSR:
     edge = np.array([x for i in range(n) for x in sorted(adj[i])], dtype=np.int32)
     degs = sorted((len(a) for a in adj), reverse=True) + [0, 0]
     return CSR(vertex, edge, degs[0], degs[1])
+
+
+def _splitmix64(x: np.ndarray) -> np.ndarray:
+    """splitmix64 finaliser over a uint64 array (counter-based, so the labels
+    of a graph do not depend on numpy's generator streams)."""
+    with np.errstate(over="ignore"):
+        z = x + np.uint64(0x9E3779B97F4A7C15)
+        z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        return z ^ (z >> np.uint64(31))
+
+
+def zipf_labels(n: int, n_labels: int, s: float, seed: int) -> np.ndarray:
+    """n labels drawn i.i.d. from Zipf(s) over 0..n_labels-1 (label k with
+    weight (k+1)^-s)."""
+    idx = np.arange(n, dtype=np.uint64) + np.uint64((seed * 0x100000001B3) & 0xFFFFFFFFFFFFFFFF)
+    u = (_splitmix64(idx) >> np.uint64(11)).astype(np.float64) / float(1 << 53)
+    w = np.arange(1, n_labels + 1, dtype=np.float64) ** (-s)
+    cdf = np.cumsum(w) / w.sum()
+    cdf[-1] = 1.0
+    return np.minimum(np.searchsorted(cdf, u, side="right"), n_labels - 1).astype(np.uint32)
+
+
+def labeled_rmat(scale: int, edge_factor: float, seed: int, keep: int, n_labels: int, zipf_s: float,
+                 label_seed: int) -> tuple[CSR, np.ndarray]:
+    """R-MAT graph restricted to the vertex ids below ``keep``, with Zipf
+    labels: the labeled FSM input (symmetric, duplicate-free)."""
+    g = rmat(scale, edge_factor, seed)
+    if keep < g.v_cnt:
+        g = restrict(g, keep)
+    return g, zipf_labels(g.v_cnt, n_labels, zipf_s, label_seed)
+
+
+def write_adj(path: str, g: CSR, labels: np.ndarray) -> None:
+    """The reference's labeled text format: first line v_cnt, then one line
+    per vertex "id label nbr nbr ..."."""
+    with open(path, "w") as f:
+        f.write(f"{g.v_cnt}\n")
+        for v in range(g.v_cnt):
+            nb = g.edge[g.vertex[v]:g.vertex[v + 1]]
+            f.write(f"{v} {int(labels[v])} " + " ".join(map(str, nb.tolist())) + "\n")

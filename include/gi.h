@@ -261,6 +261,81 @@ int gi_motif_num(int k);
 int gi_motif_patterns(int k, char *adj_out, int cap);
 int gi_motif_count(const gi_graph *g, int k, gi_stream stream, uint64_t *out_counts, int cap, gi_stats *stats);
 
+/* --------------------------------------------------- labeled graphs + FSM */
+
+/* Replaces DataLoader::load_labeled_data (reference src/dataloader.cpp:
+ * 381-625).  The input is the reference's .adj content: v_cnt vertices,
+ * each with an original label value and a neighbour list (both directions
+ * of every edge listed; self-loops are skipped as the reference skips
+ * them; duplicates are kept).  Labels are renamed 0..l_cnt-1 by descending
+ * maximum degree (first-seen order, then the reference's unstable sort for
+ * ties), vertices are renumbered by (label, -degree, id), and every
+ * neighbour list is bucketed by neighbour label.  `order` lists the vertices
+ * in the order their lines appeared (NULL = ascending id); it fixes the
+ * first-seen label order.  GI_EINVAL for an id out of range or a neighbour
+ * list that is not symmetric.  The structure is copied to the current device. */
+int gi_labeled_graph_create(int32_t v_cnt, const int64_t *vertex, const int32_t *edge, const uint32_t *labels,
+                            const int32_t *order, gi_labeled_graph **out);
+/* Parses a .adj text file: first token v_cnt, then one line per vertex
+ * "id label nbr nbr ...". */
+int gi_labeled_graph_load_adj(const char *path, gi_labeled_graph **out);
+int gi_labeled_graph_destroy(gi_labeled_graph *g);
+
+typedef struct gi_labeled_graph_info {
+    int32_t v_cnt;
+    int64_t e_cnt; /* directed entries */
+    int32_t l_cnt;
+    int32_t device;
+} gi_labeled_graph_info;
+int gi_labeled_graph_get_info(const gi_labeled_graph *g, gi_labeled_graph_info *out);
+/* Host copies of the renumbered structure: new_id[v_cnt] (original id -> new
+ * id), v_label[v_cnt], label_value[l_cnt] (original value of each new
+ * label), label_start[l_cnt+1], bucket[v_cnt*l_cnt+1] (start of the bucket
+ * of (v, l) in edge), edge[e_cnt].  Any pointer may be NULL. */
+int gi_labeled_graph_export(const gi_labeled_graph *g, int32_t *new_id, int32_t *v_label, uint32_t *label_value,
+                            uint32_t *label_start, uint32_t *bucket, uint32_t *edge);
+
+#define GI_FSM_MAX_PATTERNS 64
+/* One unlabeled pattern of an FSM run, as planned and as counted. */
+typedef struct gi_fsm_pattern {
+    int32_t n;                   /* vertices */
+    int32_t edges;
+    char adj[GI_MAX_PATTERN * GI_MAX_PATTERN]; /* '0'/'1', in schedule order */
+    int32_t n_restricts;
+    int32_t restricts[21][2];    /* (d, r): label at d <= label at r */
+    int32_t n_automorphisms;
+    int64_t jobs;                /* labeled patterns whose sub-patterns are all frequent */
+    int64_t frequent;            /* of those, with MNI support >= min_support */
+    double kernel_ms;
+} gi_fsm_pattern;
+
+typedef struct gi_fsm_stats {
+    double kernel_ms;            /* device time of the support kernels */
+    double total_ms;             /* host wall time of the whole call */
+    int64_t jobs;
+    int64_t candidates;          /* (labeled pattern, vertex, candidate) checks run */
+    int32_t kernel_launches;
+    int32_t n_patterns;          /* entries written to `patterns` */
+    gi_fsm_pattern *patterns;    /* in: optional array of GI_FSM_MAX_PATTERNS */
+} gi_fsm_stats;
+
+/* Replaces gpu_fsm's fsm_init (reference gpu/gpu_fsm.cu:779-925) and
+ * LabeledGraph::fsm (reference src/labeled_graph.cpp:540-606): the number of
+ * frequent labeled patterns with exactly max_edge edges.  Every connected
+ * pattern with at most max_edge edges is planned with the analytic model on
+ * (v_cnt, e_cnt, tri_cnt) — the reference passes a fixed triangle count per
+ * dataset (gpu_fsm: YouTube 103017122, fsm_test: Patents 7515023).  Labeled
+ * patterns are enumerated under the plan's restrictions with Apriori
+ * pruning; a labeled pattern is frequent when its MNI support (minimum over
+ * pattern vertices of the number of distinct graph vertices that vertex
+ * maps to) reaches min_support >= 1.  0 <= max_edge <= 6. */
+int gi_fsm(gi_labeled_graph *g, int max_edge, int64_t min_support, int64_t tri_cnt, gi_stream stream,
+           int64_t *out_fsm_cnt, gi_fsm_stats *stats);
+/* Plans only (no device work): fills `patterns` as gi_fsm would, with jobs
+ * and frequent left at 0. */
+int gi_fsm_plan(int max_edge, int32_t v_cnt, int64_t e_cnt, int64_t tri_cnt, gi_fsm_pattern *patterns, int cap,
+                int *count);
+
 #ifdef __cplusplus
 }
 #endif

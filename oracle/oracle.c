@@ -517,3 +517,159 @@ uint64_t oracle_triangles(const int64_t *vertex, const int32_t *edge, int32_t v_
     }
     return total;
 }
+
+/* ------------------------------------------------------------------ FSM */
+
+typedef struct {
+    int32_t v_cnt, l_cnt;
+    const uint32_t *bucket, *edge;
+    int n;
+    const int *adj;
+    const uint8_t *lab;
+    uint32_t *cand[GI_MAX_PATTERN]; /* loop set of each depth */
+    int64_t ncand[GI_MAX_PATTERN];
+    uint32_t *tmp;
+    int32_t m[GI_MAX_PATTERN];      /* matched vertices (the subtraction set) */
+    uint64_t *bits[GI_MAX_PATTERN]; /* per-position image sets */
+    int64_t count[GI_MAX_PATTERN];
+} fsm_t;
+
+static void fsm_insert(fsm_t *s, int d, uint32_t v) {
+    uint64_t *w = &s->bits[d][v >> 6];
+    const uint64_t b = (uint64_t)1 << (v & 63);
+    if (!(*w & b)) {
+        *w |= b;
+        ++s->count[d];
+    }
+}
+
+/* Loop set of depth d: the intersection of the label-d buckets of the
+ * earlier pattern neighbours of d (the chain of prefixes the reference
+ * builds for d).  Returns its size. */
+static int64_t fsm_loop_set(fsm_t *s, int d) {
+    int first = 1;
+    int64_t size = 0;
+    for (int j = 0; j < d; ++j) {
+        if (!s->adj[d * s->n + j]) continue;
+        const int64_t b = (int64_t)s->m[j] * s->l_cnt + s->lab[d];
+        const uint32_t *src = s->edge + s->bucket[b];
+        const int64_t len = (int64_t)s->bucket[b + 1] - s->bucket[b];
+        if (first) {
+            memcpy(s->cand[d], src, (size_t)len * sizeof(uint32_t));
+            size = len;
+            first = 0;
+        } else {
+            int64_t i = 0, k = 0, o = 0;
+            while (i < size && k < len) {
+                if (s->cand[d][i] < src[k]) ++i;
+                else if (s->cand[d][i] > src[k]) ++k;
+                else {
+                    s->tmp[o++] = s->cand[d][i];
+                    ++i;
+                    ++k;
+                }
+            }
+            memcpy(s->cand[d], s->tmp, (size_t)o * sizeof(uint32_t));
+            size = o;
+        }
+        if (size == 0) break;
+    }
+    s->ncand[d] = size;
+    return size;
+}
+
+static int fsm_used(const fsm_t *s, int d, uint32_t v) {
+    for (int j = 0; j < d; ++j)
+        if ((uint32_t)s->m[j] == v) return 1;
+    return 0;
+}
+
+/* Whether some embedding extends m[0..d-1]; inserts the vertices of every
+ * such embedding.  The reference skips a vertex as soon as one of the prefix
+ * sets it builds for a later depth is empty; here the later depth finds an
+ * empty loop set instead, with the same outcome. */
+static int fsm_rec(fsm_t *s, int d) {
+    if (d >= GI_MAX_PATTERN || fsm_loop_set(s, d) == 0) return 0;
+    int match = 0;
+    if (d == s->n - 1) {
+        for (int64_t i = 0; i < s->ncand[d]; ++i) {
+            const uint32_t v = s->cand[d][i];
+            if (fsm_used(s, d, v)) continue;
+            match = 1;
+            fsm_insert(s, d, v);
+        }
+        return match;
+    }
+    /* cand[d] is overwritten by deeper calls only at deeper depths */
+    for (int64_t i = 0; i < s->ncand[d]; ++i) {
+        const uint32_t v = s->cand[d][i];
+        if (fsm_used(s, d, v)) continue;
+        s->m[d] = (int32_t)v;
+        if (fsm_rec(s, d + 1)) {
+            match = 1;
+            fsm_insert(s, d, v);
+        }
+    }
+    return match;
+}
+
+int oracle_fsm_support(int32_t v_cnt, int32_t l_cnt, const uint32_t *bucket, const uint32_t *edge,
+                       const uint32_t *label_start, int n, const int *adj, int64_t n_jobs, const uint8_t *labels,
+                       int64_t min_support, int threads, int64_t *support, uint8_t *frequent) {
+    if (n < 2 || n > GI_MAX_PATTERN || v_cnt < 1 || l_cnt < 1) return -1;
+    uint32_t max_deg = 0;
+    for (int32_t v = 0; v < v_cnt; ++v) {
+        const uint32_t d = bucket[(int64_t)(v + 1) * l_cnt] - bucket[(int64_t)v * l_cnt];
+        if (d > max_deg) max_deg = d;
+    }
+    if (threads <= 0) threads = omp_get_max_threads();
+    const size_t words = ((size_t)v_cnt + 63) / 64;
+#pragma omp parallel num_threads(threads)
+    {
+        fsm_t s;
+        memset(&s, 0, sizeof(s));
+        s.v_cnt = v_cnt;
+        s.l_cnt = l_cnt;
+        s.bucket = bucket;
+        s.edge = edge;
+        s.n = n;
+        s.adj = adj;
+        for (int d = 0; d < n; ++d) {
+            s.cand[d] = (uint32_t *)malloc(((size_t)max_deg + 1) * sizeof(uint32_t));
+            s.bits[d] = (uint64_t *)malloc(words * sizeof(uint64_t));
+        }
+        s.tmp = (uint32_t *)malloc(((size_t)max_deg + 1) * sizeof(uint32_t));
+#pragma omp for schedule(dynamic, 1)
+        for (int64_t j = 0; j < n_jobs; ++j) {
+            s.lab = labels + j * n;
+            for (int d = 0; d < n; ++d) {
+                memset(s.bits[d], 0, words * sizeof(uint64_t));
+                s.count[d] = 0;
+            }
+            int64_t sup = v_cnt;
+            int any = 0;
+            const uint32_t end = label_start[s.lab[0] + 1];
+            for (uint32_t v = label_start[s.lab[0]]; v < end; ++v) {
+                s.m[0] = (int32_t)v;
+                if (!fsm_rec(&s, 1)) continue;
+                any = 1;
+                fsm_insert(&s, 0, v);
+                sup = v_cnt;
+                for (int d = 0; d < n; ++d)
+                    if (s.count[d] < sup) sup = s.count[d];
+                if (sup >= min_support) break;
+            }
+            sup = v_cnt;
+            for (int d = 0; d < n; ++d)
+                if (s.count[d] < sup) sup = s.count[d];
+            support[j] = sup;
+            frequent[j] = (uint8_t)(any && sup >= min_support);
+        }
+        for (int d = 0; d < n; ++d) {
+            free(s.cand[d]);
+            free(s.bits[d]);
+        }
+        free(s.tmp);
+    }
+    return 0;
+}

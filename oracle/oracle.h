@@ -70,6 +70,26 @@ uint64_t oracle_clique_count(int k, const int64_t *vertex, const int32_t *edge, 
  * reference src/graph.cpp:1006-1043 (motif_counting_3). */
 uint64_t oracle_triangles(const int64_t *vertex, const int32_t *edge, int32_t v_cnt, int threads);
 
+/* MNI support of labeled patterns by the reference's CPU enumeration
+ * (reference src/labeled_graph.cpp:120-353, get_support_pattern_matching and
+ * get_support_pattern_matching_aggressive_func, with the loop sets of
+ * Schedule_IEP::update_loop_invariant_for_fsm, src/schedule_IEP.cpp:393-418):
+ * for every start vertex of label[0], every embedding below it is
+ * enumerated (in the schedule's vertex order; the loop set of depth d is the
+ * intersection of the label-d buckets of its earlier neighbours, minus the
+ * vertices already matched), the vertices of each complete embedding go into
+ * per-position sets, and the scan stops once the smallest set holds
+ * min_support vertices.  Graph: the bucketed structure of the reference
+ * loader (bucket[v*l_cnt+l] .. bucket[v*l_cnt+l+1] in edge are v's
+ * neighbours with label l; label_start[l] .. label_start[l+1] the vertices
+ * with label l).  Pattern: n vertices, adj n*n 0/1 ints in schedule order.
+ * labels[j*n + i] is job j's label of position i.  support[j] receives the
+ * support at the point the scan stopped, frequent[j] = support >= min_support
+ * and at least one embedding found.  Returns 0, or -1 on bad input. */
+int oracle_fsm_support(int32_t v_cnt, int32_t l_cnt, const uint32_t *bucket, const uint32_t *edge,
+                       const uint32_t *label_start, int n, const int *adj, int64_t n_jobs, const uint8_t *labels,
+                       int64_t min_support, int threads, int64_t *support, uint8_t *frequent);
+
 #ifdef __cplusplus
 }
 #endif

@@ -71,3 +71,26 @@ def plan_desc(schedule):
     d = N.PlanDesc()
     N.check(N.lib().gi_plan_export(schedule.handle, C.byref(d)), "gi_plan_export")
     return d
+
+
+@pytest.fixture(scope="session")
+def golden_fsm():
+    with open(GOLDEN / "fsm.json") as f:
+        return json.load(f)
+
+
+@pytest.fixture(scope="session")
+def fsm_graphs(golden_fsm, native, tmp_path_factory):
+    """The seeded labeled graphs behind fsm.json: name -> (CSR, labels, path of
+    the regenerated .adj file), each checked against its recorded sha1."""
+    import hashlib
+    from graphindor_b200 import gen
+    d = tmp_path_factory.mktemp("fsm")
+    out = {}
+    for name, meta in golden_fsm["graphs"].items():
+        g, labels = gen.labeled_rmat(**meta["params"])
+        path = d / f"{name}.adj"
+        gen.write_adj(str(path), g, labels)
+        assert hashlib.sha1(path.read_bytes()).hexdigest() == meta["adj_sha1"], f"generator drift for {name}"
+        out[name] = (g, labels, path)
+    return out

@@ -12,7 +12,10 @@ Writes
                 stored as (length, sha1, first 256 entries);
   counts.json   reference pm_test / clique_test / motif_counting_test counts on
                 seeded synthetic graphs, with each graph's generator parameters
-                and a sha1 of its CSR arrays so tests can regenerate it.
+                and a sha1 of its CSR arrays so tests can regenerate it;
+  fsm.json      reference fsm_test results on seeded labeled graphs (generator
+                parameters, sha1 of the .adj text) and the reference planner's
+                FSM schedules for each graph.
 
 The tests never read the reference; they only read these files.
 """
@@ -160,15 +163,95 @@ def write_counts(motifs):
         json.dump(out, f, indent=1, sort_keys=True)
 
 
+# Labeled graphs for FSM: (scale, edge_factor, seed, keep, n_labels, zipf_s,
+# label_seed) of graphindor_b200.gen.labeled_rmat, and the (max_edge,
+# min_support) runs of the reference fsm_test on each.
+FSM_GRAPHS = {
+    "lrmat_s10_l5": (dict(scale=10, edge_factor=8.0, seed=5, keep=900, n_labels=5, zipf_s=1.1, label_seed=7),
+                     [(me, ms) for me in (1, 2, 3) for ms in (5, 20, 60)] + [(4, 40)]),
+    "lrmat_s11_l12": (dict(scale=11, edge_factor=10.0, seed=21, keep=1800, n_labels=12, zipf_s=1.1, label_seed=8),
+                      [(me, ms) for me in (2, 3) for ms in (10, 40)]),
+    "lrmat_s12_l29": (dict(scale=12, edge_factor=12.0, seed=31, keep=3500, n_labels=29, zipf_s=1.1, label_seed=9),
+                      [(me, ms) for me in (2, 3) for ms in (15, 50)]),
+    "lrmat_s12_l3": (dict(scale=12, edge_factor=6.0, seed=41, keep=4096, n_labels=3, zipf_s=0.3, label_seed=10),
+                     [(3, 200), (3, 800)]),
+}
+FSM_TRI_CNT = 7515023  # fsm_test plans with the Patents constant (reference src/fsm_test.cpp:27)
+
+
+def adj_sha1(path: Path) -> str:
+    return hashlib.sha1(path.read_bytes()).hexdigest()
+
+
+def fsm_plans(motifs_by_k, max_edge, v_cnt, e_cnt):
+    """The reference's FSM plans: Schedule_IEP(p, valid, 1, 1, 1, v, e, tri)
+    of every connected pattern with at most max_edge edges (reference
+    src/labeled_graph.cpp:180-196, :438-452), as (schedule-order adjacency,
+    label restrictions (d, r))."""
+    pats = []
+    for k in range(2, max_edge + 2):
+        for adj in motifs_by_k[k]:
+            e = sum(adj[i * k + j] == "1" for i in range(k) for j in range(i + 1, k))
+            if e <= max_edge:
+                pats.append((e, k, adj))
+    pats.sort(key=lambda t: t[0])  # stable
+    jobs = [f"full {k} {adj} {v_cnt} {e_cnt} {FSM_TRI_CNT} 1" for _, k, adj in pats]
+    res = subprocess.run([str(REF_BIN / "ref_plan_dump")], input="\n".join(jobs) + "\n", capture_output=True,
+                         text=True, check=True).stdout.splitlines()
+    out = []
+    for (e, k, _), line in zip(pats, res):
+        d = json.loads(line)
+        restricts = []
+        for depth in range(k):
+            r = d["restrict_last"][depth]
+            while r != -1:
+                restricts.append([depth, d["restrict_index"][r]])
+                r = d["restrict_next"][r]
+        out.append({"n": k, "edges": e, "adj": "".join(str(x) for x in d["adj_mat"]), "restricts": restricts})
+    return out
+
+
+def write_fsm():
+    motifs_by_k = {}
+    lines = subprocess.run([str(REF_BIN / "ref_plan_dump")], input="".join(f"motifs {k} -\n" for k in range(2, 6)),
+                           capture_output=True, text=True, check=True).stdout.splitlines()
+    for k, line in zip(range(2, 6), lines):
+        motifs_by_k[k] = json.loads(line)["motifs"]
+    out = {"tri_cnt": FSM_TRI_CNT, "graphs": {}}
+    with tempfile.TemporaryDirectory() as td:
+        for name, (params, runs) in FSM_GRAPHS.items():
+            g, labels = gen.labeled_rmat(**params)
+            path = Path(td) / f"{name}.adj"
+            gen.write_adj(str(path), g, labels)
+            e_cnt = int(g.e_cnt)
+            max_me = max(me for me, _ in runs)
+            rows = []
+            for me, ms in runs:
+                t = time.time()
+                txt = run_ref("fsm_test", path, me, ms)
+                cnt = int(re.findall(r"fsm_cnt = (-?\d+)", txt)[-1])
+                rows.append({"max_edge": me, "min_support": ms, "fsm_cnt": cnt})
+                print(name, me, ms, cnt, f"{time.time() - t:.2f}s", flush=True)
+            out["graphs"][name] = {"params": params, "v_cnt": g.v_cnt, "e_cnt": e_cnt, "adj_sha1": adj_sha1(path),
+                                   "runs": rows, "plans": fsm_plans(motifs_by_k, max_me, g.v_cnt, e_cnt)}
+    with open(HERE / "fsm.json", "w") as f:
+        json.dump(out, f, indent=1, sort_keys=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default="/root/reference")
     ap.add_argument("--skip-plans", action="store_true")
+    ap.add_argument("--only-fsm", action="store_true")
     a = ap.parse_args()
+    if a.only_fsm:
+        write_fsm()
+        return
     jobs, motifs = plan_jobs(Path(a.ref))
     if not a.skip_plans:
         write_plans(jobs)
     write_counts(motifs)
+    write_fsm()
 
 
 if __name__ == "__main__":
