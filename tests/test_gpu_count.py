@@ -204,3 +204,27 @@ def test_edge_cases(oracle):
             s = gi.Schedule_IEP(gi.Pattern(n, adj), g.v_cnt, g.e_cnt, 0, model=2)
             assert gi.pattern_matching(dg, s).count == oracle.brute(n, adj, g.vertex, g.edge)
         assert gi.clique_count(dg, 3, 0).count == 0 or g is not star
+
+
+def test_distributed_count_over_nccl_matches_the_single_gpu_count(golden_graphs, dev_graphs):
+    """World size 1 over NCCL: the shard count plus the 2^64 all-reduce."""
+    import datetime
+    import os
+    import socket
+    import torch
+    import torch.distributed as dist
+    from graphindor_b200 import distributed as gd
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    os.environ["MASTER_ADDR"], os.environ["MASTER_PORT"] = "127.0.0.1", str(port)
+    torch.cuda.set_device(0)
+    dist.init_process_group("nccl", rank=0, world_size=1, timeout=datetime.timedelta(seconds=60))
+    try:
+        g, dg = golden_graphs["rmat_s10_ef12"], dev_graphs["rmat_s10_ef12"]
+        for n, adj in [(4, "0110100110010110"), (5, "0101110101010101010011000")]:
+            s = gi.Schedule_IEP(gi.Pattern(n, adj), g.v_cnt, g.e_cnt, 0)
+            assert gd.count(dg, s) == gi.pattern_matching(dg, s).count
+        assert gd.allreduce_u64([(1 << 64) - 1]) == [(1 << 64) - 1]
+    finally:
+        dist.destroy_process_group()
