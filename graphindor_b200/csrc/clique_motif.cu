@@ -3,7 +3,8 @@
 // gi_clique_count: the graph is oriented into a DAG on the device, then the
 // clique plan (Schedule_IEP(adj_mat, k): every position adjacent to every
 // earlier one, no restrictions, no IEP) runs through the counting kernel
-// over the DAG's edges.  orientation 0 keeps u -> v when v < u (reference
+// over the DAG's edges — or, for the degree orientation, the per-vertex
+// bitmap kernels of kclique.cu.  orientation 0 keeps u -> v when v < u (reference
 // reduce_edges_for_clique, src/graph.cpp:710-735, used by gpu/gpu_clique.cu
 // :585 and src/clique_test.cpp:73); orientation 1 keeps u -> v when
 // (deg u, u) < (deg v, v) (reference degree_orientation_init,
@@ -28,6 +29,8 @@ int cuda_fail(cudaError_t e, const char *what);
 int count_impl(gi_graph *g, const DevPlan &P, cudaStream_t st, uint64_t *raw_sum, gi_stats *stats, double budget_ms,
                int64_t shard, int64_t num_shards);
 void graph_free(gi_graph *g);
+int kclique_bitmap(gi_graph *o, int k, cudaStream_t st, uint64_t *out, gi_stats *stats);
+int kclique_max_bitmap_degree();
 
 namespace {
 
@@ -192,6 +195,14 @@ extern "C" int gi_clique_count(const gi_graph *cg, int k, int orientation, gi_st
         return GI_OK;
     }
     std::lock_guard<std::mutex> lock2(o->mu);
+    // Degree orientation: per-vertex bitmaps (kclique.cu) unless an
+    // out-degree is too large for them or the caller asked for a work budget
+    // or byte accounting, which only the general kernel provides.
+    if (orientation == 1 && o->max_degree <= kclique_max_bitmap_degree() && budget <= 0 &&
+        !(stats && stats->count_bytes)) {
+        rc = kclique_bitmap(o, k, st, out_count, stats);
+        if (rc != GI_ENOMEM) return rc;  // bitmaps too large for free memory: general kernel below
+    }
     rc = count_impl(o, plan->dev, st, &raw, stats, budget, 0, 1);
     if (rc != GI_OK) return rc;
     *out_count = raw;  // redundancy is 1 for the clique plan (reference gpu/gpu_clique.cu:628)

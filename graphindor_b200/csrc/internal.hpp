@@ -93,4 +93,10 @@ struct gi_graph {
     size_t scan_tmp_bytes = 0;
     // Lazily built derived graphs (clique orientations).
     gi_graph *oriented[2] = {nullptr, nullptr};
+    // Per-vertex adjacency bitmaps of a degree-oriented DAG (kclique.cu),
+    // built by the first k-clique count and kept: row i of vertex u has bit j
+    // when out-neighbour j of u is an out-neighbour of out-neighbour i.
+    uint32_t *d_bitmap = nullptr;
+    int64_t *d_bitmap_off = nullptr;  // v_cnt + 1 word offsets
+    int64_t bitmap_words = 0;
 };

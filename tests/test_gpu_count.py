@@ -228,3 +228,32 @@ def test_distributed_count_over_nccl_matches_the_single_gpu_count(golden_graphs,
         assert gd.allreduce_u64([(1 << 64) - 1]) == [(1 << 64) - 1]
     finally:
         dist.destroy_process_group()
+
+
+def _complete(n):
+    return gen.from_edges(n, [(i, j) for i in range(n) for j in range(i + 1, n)])
+
+
+def test_kclique_bitmaps_match_the_dfs_path_and_closed_forms(oracle):
+    """Degree orientation runs the bitmap kernels (kclique.cu): rows of up to
+    four words one per lane, longer rows (out-degree > 128) one per warp, lists
+    over 1024 entries searched in global memory.  They must equal the general
+    kernel on the same DAG and on the id DAG, the oracle's triangles, and
+    C(n, k) on complete graphs."""
+    from math import comb
+    g = gen.chung_lu(10000, 800000, 1.9, 3000.0, 17)  # out-degrees up to 208
+    deg = np.diff(g.vertex)
+    src = np.repeat(np.arange(g.v_cnt), deg)
+    dst = g.edge.astype(np.int64)
+    keep = (deg[src] < deg[dst]) | ((deg[src] == deg[dst]) & (src < dst))
+    assert np.bincount(src[keep], minlength=g.v_cnt).max() > 128  # both tiers run
+    dg = gi.Graph.from_csr(g.vertex, g.edge)
+    assert gi.clique_count(dg, 3, 1).count == oracle.triangles(g.vertex, g.edge)
+    for k in (3, 4, 5):
+        bitmap = gi.clique_count(dg, k, 1)
+        dfs = gi.clique_count(dg, k, 1, count_bytes=True)  # byte accounting forces the general kernel
+        assert bitmap.count == dfs.count == gi.clique_count(dg, k, 0).count, k
+    for n, ks in ((40, (3, 4, 5, 6, 7)), (300, (3, 4, 5)), (1100, (3, 4))):
+        dg = gi.Graph.from_csr(*(lambda c: (c.vertex, c.edge))(_complete(n)))
+        for k in ks:
+            assert gi.clique_count(dg, k, 1).count == comb(n, k) % (1 << 64), (n, k)
