@@ -8,17 +8,17 @@ planned as the reference's gpu_graph plans them (analytic model, the
 reference's restriction generator, IEP on).
 
 The whole six-pattern job runs for days on any machine, so the bench
-measures random samples of it.  First-level work is cut into chunks of
-GI_TASK_CHUNK subtasks; a step counts, for every pattern, shard
-(step * world + rank) mod NSHARD of NSHARD with a device time budget: the
-shard's chunks are visited in a fixed pseudo-random order, no chunk starts
-after BUDGET_MS and chunks still running at 3 * BUDGET_MS are dropped, so
-the completed chunks (fraction f_p of the pattern's job) are a random
-sample of its work.
+measures a fixed random sample of it.  First-level work is cut into chunks of
+GI_TASK_CHUNK subtasks; for pattern p a step counts the first M_p chunks of a
+fixed pseudo-random order over all of them (gi_stats.sample_chunks), each to
+completion, with M_p = SAMPLE_CHUNKS[p].  The sample, and so its count, is the
+same on every run; only the time varies.  Under torchrun rank r samples shard r of
+world (weak scaling: every rank counts its own M_p chunks).
 
 value = whole-job throughput estimated from the samples:
           sum_p (embeddings counted for p) / f_p  over  sum_p (device time for p) / f_p
-        with the graph resident in HBM (device time from CUDA events).
+        with f_p = M_p / chunks_p and the graph resident in HBM (device time
+        from CUDA events).
 e2e   = the same whole job through the public API from pinned host buffers:
         graph upload (H2D) + planning + counts + result reads (D2H).
 cpu_baseline / --impl reference: the reference's CPU path (the oracle, a C
@@ -53,8 +53,12 @@ PATTERNS = [
     ("prism", 6, "011100101010110001100011010101001110"),
     ("6-cycle+chord", 6, "010101101000010100101010000101100010"),
 ]
-NSHARD = 16                  # each step samples a different 1/16 of the chunks
-BUDGET_MS = 1000.0           # device time budget of one pattern's sample
+# Chunks of each pattern's fixed sample (0 = all of them).  Sized on a B200 at
+# scale 22 so that each sample takes about 0.5 - 7 s: the prism and 6-cycle +
+# chord jobs are so heavy-tailed (5.8e6 and ~1e8 device-seconds whole) that 64
+# and 16 chunks already take seconds; their estimates are the roughest.
+SAMPLE_CHUNKS = {"diamond": 0, "4-cycle": 65536, "house": 16384, "5-clique": 16384, "prism": 64,
+                 "6-cycle+chord": 16}
 CPU_TARGET_S = 3.0           # host time of one pattern's CPU slice
 MEASURED = ROOT / "MEASURED_PEAKS.json"
 METRIC = "pattern-match embeddings/s, whole six-pattern job (R-MAT s22, IEP), 1 B200"
@@ -68,7 +72,7 @@ def parse_args():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--scale", type=int, default=SCALE)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--budget-ms", type=float, default=BUDGET_MS)
+    ap.add_argument("--sample-scale", type=float, default=1.0, help="multiplies every sample size")
     ap.add_argument("--cpu-target-s", type=float, default=CPU_TARGET_S)
     return ap.parse_args()
 
@@ -147,16 +151,27 @@ def run_ours(args, world, rank, local):
     plans = {name: gi.Schedule_IEP(gi.Pattern(n, adj), dg.v_cnt, dg.e_cnt, tri) for name, n, adj in PATTERNS}
     divisors = {name: plans[name].export()["count_divisor"] for name, _, _ in PATTERNS}
 
+    # Chunks per pattern (shard `rank` of `world`), then the fixed sample sizes.
+    sample = {}
+    for name, _, _ in PATTERNS:
+        st = N.Stats()
+        st.sample_chunks = 1
+        raw = C.c_uint64()
+        N.check(L.gi_count_shard(dg.handle, plans[name].handle, rank, world, sp, C.byref(raw), C.byref(st)),
+                "gi_count_shard")
+        want = SAMPLE_CHUNKS[name]
+        m = st.chunks_total if want == 0 else max(1, int(round(want * args.sample_scale)))
+        sample[name] = (min(m, st.chunks_total), st.chunks_total)
+
     def one_step(graph, plan_map, step, acc, count_bytes=False):
         for name, _, _ in PATTERNS:
             st = N.Stats()
             st.count_bytes = 1 if count_bytes else 0
-            st.budget_ms = args.budget_ms
-            st.allow_partial = 1
+            st.sample_chunks = sample[name][0]
             raw = C.c_uint64()
-            N.check(L.gi_count_shard(graph.handle, plan_map[name].handle, (step * world + rank) % NSHARD, NSHARD, sp,
-                                     C.byref(raw), C.byref(st)), "gi_count_shard")
-            f = st.chunks_done / max(1, st.chunks_total * NSHARD)  # fraction of the whole job
+            N.check(L.gi_count_shard(graph.handle, plan_map[name].handle, rank, world, sp, C.byref(raw),
+                                     C.byref(st)), "gi_count_shard")
+            f = st.chunks_done / max(1, st.chunks_total * world)  # fraction of the whole job
             a = acc.setdefault(name, {"emb": 0.0, "ms": 0.0, "launches": 0, "bytes_per_chunk": 0.0, "chunks": 0,
                                       "job_emb": 0.0, "job_ms": 0.0, "prep_ms": 0.0})
             a["emb"] += raw.value / divisors[name]
@@ -179,8 +194,7 @@ def run_ours(args, world, rank, local):
     for s in range(args.warmup):
         one_step(dg, plans, s, {})
     instr = {}
-    for s in steps:  # algorithmic bytes of the timed shards (instrumented pass, untimed)
-        one_step(dg, plans, s, instr, count_bytes=True)
+    one_step(dg, plans, 0, instr, count_bytes=True)  # algorithmic bytes of the (fixed) sample, untimed
 
     clocks = Clocks(torch.cuda.current_device())
     barrier()
@@ -260,8 +274,9 @@ def run_ours(args, world, rank, local):
         "config": {
             "workload": f"R-MAT scale {args.scale}, edge factor {EDGE_FACTOR}, seed {SEED}: {g.v_cnt} vertices, "
                         f"{g.e_cnt // 2} undirected edges; six patterns with IEP, reference plans; whole-job "
-                        f"throughput estimated from time-budgeted random samples ({args.budget_ms:.0f} ms per "
-                        f"pattern per step, 1/{NSHARD} shard per step)",
+                        f"throughput estimated from a fixed seeded random sample of each pattern's work chunks "
+                        f"(the same sample every step and run)",
+            "sample_chunks": {n: {"sampled": sample[n][0], "of": sample[n][1]} for n in names},
             "patterns": {n: adj for n, _, adj in PATTERNS},
             "per_pattern_job_s_estimate": {n: job_ms_p[n] / 1e3 / args.steps for n in names},
             "per_pattern_embeddings_estimate": {n: job_emb_p[n] / args.steps for n in names},

@@ -67,6 +67,10 @@ __global__ void split_count_kernel(const __grid_constant__ DevPlan P, const int6
 // of dependent loads and gain from the extra resident warps despite some
 // spilling (R-MAT scale 22: prism 1.6x, 6-cycle+chord 1.6x faster at 16
 // blocks); shallower plans run best with the unconstrained allocation.
+constexpr unsigned kTakerSpins = 1u << 20;  // empty polls of ~2 us before an idle warp leaves
+constexpr unsigned kReadySpins = 1u << 22;  // polls of a claimed item's ready flag
+constexpr unsigned long long kHandoffCap = 1ull << 20;
+
 template <bool kBytesOn, int kMinBlocks>
 __global__ void __launch_bounds__(kBlockThreads, kMinBlocks)
     dfs_count_kernel(const __grid_constant__ DevPlan P, const int64_t *__restrict__ vertex,
@@ -74,7 +78,8 @@ __global__ void __launch_bounds__(kBlockThreads, kMinBlocks)
                      const int64_t *__restrict__ offsets, int64_t n_tasks, int split, uint32_t *scratch,
                      int64_t slot_stride, unsigned long long *counters, unsigned long long budget_ns, int64_t shard,
                      int64_t num_shards, int64_t n_chunks, int64_t perm_a, int64_t perm_b,
-                     unsigned long long hard_ns) {
+                     unsigned long long hard_ns, unsigned long long max_claims, Handoff *hitems,
+                     unsigned long long hcap, uint32_t hepoch, uint32_t v_cnt) {
     __shared__ WarpState states[kWarpsPerBlock];
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
@@ -86,6 +91,13 @@ __global__ void __launch_bounds__(kBlockThreads, kMinBlocks)
     const unsigned long long t_start = globaltimer();
     c.t_start = t_start;
     c.hard_ns = hard_ns;
+    if (hitems) {
+        c.hq.items = hitems;
+        c.hq.cap = hcap;
+        c.hq.ctr = counters + kQueue;
+        c.hq.epoch = hepoch;
+        c.hq.v_cnt = v_cnt;
+    }
     while (true) {
         // Claim the next chunk of kTaskChunk consecutive work items of this
         // shard: slot shard + j * num_shards (the reference's static
@@ -96,7 +108,9 @@ __global__ void __launch_bounds__(kBlockThreads, kMinBlocks)
         int stop = 0;
         if (lane == 0) {
             j = atomicAdd(&counters[kCursor], 1ull);
-            if (budget_ns && globaltimer() - t_start > budget_ns) {
+            if (max_claims && j >= max_claims) {
+                stop = 1;  // a fixed sample: the first max_claims chunks of the order
+            } else if (budget_ns && globaltimer() - t_start > budget_ns) {
                 timed_out = true;
                 stop = 1;
             }
@@ -174,8 +188,67 @@ __global__ void __launch_bounds__(kBlockThreads, kMinBlocks)
         tasks += chunk_tasks;
         ++chunks;
     }
+    // Out of chunks: take handed-off ranges until every warp is idle or gone
+    // and the queue is empty.  Waits are bounded: an idle warp gives up after
+    // kTakerSpins empty polls (items still queued then are drained by the
+    // warps that queued them, which poll before they leave), and a taken item
+    // whose ready flag never appears is recorded in kLost.
+    bool lost = false;
+    const bool warp_timed_out = __shfl_sync(kFull, timed_out ? 1 : 0, 0) != 0;
+    if (hitems && warp_timed_out && lane == 0) atomicAdd(&counters[kQueue + 3], 1ull);  // gone
+    if (hitems && !warp_timed_out) {
+        unsigned long long *qc = counters + kQueue;  // head, tail, idle, exited
+        const unsigned long long total = static_cast<unsigned long long>(gridDim.x) * kWarpsPerBlock;
+        if (lane == 0) atomicAdd(&qc[2], 1ull);
+        unsigned spins = 0;
+        while (true) {
+            long long slot = -1;
+            int quit = 0;
+            if (lane == 0) {
+                const unsigned long long h = *(volatile unsigned long long *)&qc[0];
+                const unsigned long long t = *(volatile unsigned long long *)&qc[1];
+                if (h < (t < hcap ? t : hcap)) {
+                    atomicAdd(&qc[2], ~0ull);  // busy unless the claim fails
+                    if (atomicCAS(&qc[0], h, h + 1) == h)
+                        slot = static_cast<long long>(h);
+                    else
+                        atomicAdd(&qc[2], 1ull);
+                } else {
+                    const unsigned long long idle = *(volatile unsigned long long *)&qc[2];
+                    const unsigned long long gone = *(volatile unsigned long long *)&qc[3];
+                    if (idle + gone >= total || ++spins > kTakerSpins)
+                        quit = 1;
+                    else
+                        __nanosleep(2000);
+                }
+            }
+            slot = __shfl_sync(kFull, slot, 0);
+            if (__shfl_sync(kFull, quit, 0)) break;
+            if (slot < 0) continue;
+            int ready = 0;
+            if (lane == 0) {
+                for (unsigned k = 0; k < kReadySpins && !ready; ++k) {
+                    ready = *(volatile uint32_t *)&hitems[slot].ready == hepoch;
+                    if (!ready) __nanosleep(64);
+                }
+                __threadfence();
+            }
+            unsigned long long part = 0;
+            if (__shfl_sync(kFull, ready, 0) && slot < static_cast<long long>(hcap) && c.run_handoff(&hitems[slot], part))
+                sum += part;
+            else
+                lost = true;
+            if (lane == 0) atomicAdd(&qc[2], 1ull);
+            spins = 0;
+        }
+        if (lane == 0) {
+            atomicAdd(&qc[2], ~0ull);
+            atomicAdd(&qc[3], 1ull);
+        }
+    }
     const unsigned long long lane_bytes = kBytesOn ? warp_sum(c.bytes) : 0;
     if (lane == 0) {
+        if (lost) atomicAdd(&counters[kLost], 1ull);
         atomicAdd(&counters[kSum], sum);
         atomicAdd(&counters[kTasks], tasks);
         atomicAdd(&counters[kChunks], chunks);
@@ -203,7 +276,13 @@ int ensure_scratch(gi_graph *g, size_t bytes) {
 
 // Candidates of the depth-2 loop per subtask: one lane each when depth 2 is
 // the leaf level, one warp at a time otherwise.
-static int split_size(const DevPlan &P) { return P.leaf_depth == 2 ? 256 : 32; }
+#ifndef GI_SPLIT_LEAF2
+#define GI_SPLIT_LEAF2 256
+#endif
+#ifndef GI_SPLIT_DEEP
+#define GI_SPLIT_DEEP 32
+#endif
+static int split_size(const DevPlan &P) { return P.leaf_depth == 2 ? GI_SPLIT_LEAF2 : GI_SPLIT_DEEP; }
 
 // Builds the subtask offsets for the plan's depth-2 split; returns the
 // number of subtasks.  Caller holds g->mu.
@@ -295,19 +374,23 @@ int count_impl(gi_graph *g, const DevPlan &P, cudaStream_t st, uint64_t *raw_sum
         }
         launches += 1;  // split count (the scan is cub's)
     }
-    if ((e = cudaMemsetAsync(g->d_counters, 0, 8 * sizeof(unsigned long long), st)) != cudaSuccess)
+    if ((e = cudaMemsetAsync(g->d_counters, 0, kCounterSlots * sizeof(unsigned long long), st)) != cudaSuccess)
         return cuda_fail(e, "counter reset");
     // Work budget: each warp stops claiming work once %globaltimer has
     // advanced budget_ns past its own start, and the call reports
     // GI_ETIMEOUT.  No wait in the kernel depends on another warp.  A
     // sampled count (allow_partial) visits the chunks in a pseudo-random
     // order and drops chunks still running at three times the budget.
+    // A fixed sample (sample_chunks) visits the same pseudo-random order and
+    // stops claiming after that many chunks, each counted to completion.
     const unsigned long long budget_ns = budget_ms > 0 ? static_cast<unsigned long long>(budget_ms * 1e6) : 0ull;
     const bool partial = budget_ns && stats && stats->allow_partial;
+    const unsigned long long max_claims =
+        stats && stats->sample_chunks > 0 ? static_cast<unsigned long long>(stats->sample_chunks) : 0ull;
     const int64_t *offs = use_split ? g->d_offsets : nullptr;
     const int64_t n_chunks = (n_tasks + kTaskChunk - 1) / kTaskChunk;
     int64_t perm_a = 0, perm_b = 0;
-    if (partial && n_chunks > 1) {
+    if ((partial || max_claims) && n_chunks > 1) {
         perm_a = static_cast<int64_t>(2654435761ull % static_cast<unsigned long long>(n_chunks));
         auto gcd = [](int64_t x, int64_t y) {
             while (y) {
@@ -322,15 +405,32 @@ int count_impl(gi_graph *g, const DevPlan &P, cudaStream_t st, uint64_t *raw_sum
         perm_b = n_chunks / 3;
     }
     const unsigned long long hard_ns = partial ? 3ull * budget_ns : 0ull;
+    // Work donation, except in time-budgeted samples (whose dropped chunks
+    // must take their handed-off ranges with them).
+    Handoff *hitems = nullptr;
+    if (!hard_ns) {
+        if (!g->d_handoff) {
+            if ((e = cudaMalloc(&g->d_handoff, kHandoffCap * sizeof(Handoff))) != cudaSuccess ||
+                (e = cudaMemsetAsync(g->d_handoff, 0, kHandoffCap * sizeof(Handoff), st)) != cudaSuccess) {
+                cudaFree(g->d_handoff);
+                g->d_handoff = nullptr;
+                return cuda_fail(e, "handoff queue allocation");
+            }
+        }
+        hitems = static_cast<Handoff *>(g->d_handoff);
+        if (++g->handoff_epoch == 0) ++g->handoff_epoch;
+    }
     cudaEventRecord(tm, st);
     kernel<<<blocks, kBlockThreads, 0, st>>>(P, g->d_vertex, reinterpret_cast<const uint32_t *>(g->d_edge),
                                              g->d_edge_from, g->e_cnt, offs, n_tasks, split,
                                              static_cast<uint32_t *>(g->d_scratch), stride, g->d_counters, budget_ns,
-                                             shard, num_shards, n_chunks, perm_a, perm_b, hard_ns);
+                                             shard, num_shards, n_chunks, perm_a, perm_b, hard_ns, max_claims,
+                                             hitems, kHandoffCap, g->handoff_epoch,
+                                             static_cast<uint32_t>(g->v_cnt));
     launches += 1;
     e = cudaGetLastError();
     cudaEventRecord(t1, st);
-    unsigned long long host[8] = {0};
+    unsigned long long host[kCounterSlots] = {0};
     if (e == cudaSuccess) e = cudaMemcpyAsync(host, g->d_counters, sizeof(host), cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     float ms = 0.f, prep = 0.f;
@@ -342,6 +442,7 @@ int count_impl(gi_graph *g, const DevPlan &P, cudaStream_t st, uint64_t *raw_sum
     cudaEventDestroy(tm);
     cudaEventDestroy(t1);
     if (e != cudaSuccess) return cuda_fail(e, "counting kernel");
+    if (host[kLost]) return fail(GI_ECUDA, "a handed-off work item was never published");
     if (host[kTimeout] && !partial) return fail(GI_ETIMEOUT, "count exceeded its device time budget");
     *raw_sum = host[kSum];
     if (stats) {
@@ -369,11 +470,13 @@ static void reset_stats(gi_stats *stats, double &budget) {
     if (!stats) return;
     const int cb = stats->count_bytes;
     const int partial = stats->allow_partial;
+    const int64_t sample = stats->sample_chunks;
     budget = stats->budget_ms;
     std::memset(stats, 0, sizeof(*stats));
     stats->count_bytes = cb;
     stats->budget_ms = budget;
     stats->allow_partial = partial;
+    stats->sample_chunks = sample;
 }
 
 extern "C" int gi_count(const gi_graph *cg, const gi_plan *p, gi_stream stream, uint64_t *out_count,
@@ -384,6 +487,10 @@ extern "C" int gi_count(const gi_graph *cg, const gi_plan *p, gi_stream stream, 
     uint64_t raw = 0;
     double budget = 0.0;
     reset_stats(stats, budget);
+    if (stats) {  // samples are a gi_count_shard feature; a whole count is whole
+        stats->allow_partial = 0;
+        stats->sample_chunks = 0;
+    }
     const int st = count_impl(g, p->dev, static_cast<cudaStream_t>(stream), &raw, stats, budget, 0, 1);
     if (st != GI_OK) return st;
     if (stats && stats->count_bytes) {

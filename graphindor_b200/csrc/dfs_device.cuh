@@ -20,8 +20,10 @@ constexpr int kBlockThreads = kWarpsPerBlock * 32;
 constexpr int kTaskChunk = GI_TASK_CHUNK;
 constexpr unsigned kFull = 0xffffffffu;
 
-// Counter slots in gi_graph::d_counters.
-enum : int { kSum = 0, kCursor = 1, kBytes = 2, kTasks = 3, kTimeout = 4, kChunks = 5 };
+// Counter slots in gi_graph::d_counters; kQueue.. kQueue+3 are the handoff
+// queue's head, tail, idle-warp and exited-warp counters.
+enum : int { kSum = 0, kCursor = 1, kBytes = 2, kTasks = 3, kTimeout = 4, kChunks = 5, kQueue = 6, kLost = 10 };
+constexpr int kCounterSlots = 16;
 
 struct WarpState {
     const uint32_t *set_ptr[GI_MAX_PREFIX];
@@ -32,6 +34,35 @@ struct WarpState {
     int32_t end[GI_MAX_PATTERN + 1];
     uint32_t minv[GI_MAX_PATTERN + 1];
 };
+
+// Work donation: a warp with a long loop range hands the upper half to an
+// idle warp through a queue in device memory.  An item is the partial
+// embedding emb[0, depth) and a range [lo, hi) of depth's loop set; the taker
+// rebuilds the prefix sets from the embedding (the same sets, built the same
+// way) and runs the range.
+struct Handoff {
+    uint32_t emb[GI_MAX_PATTERN];
+    int32_t depth;
+    int32_t lo;
+    int32_t hi;
+    uint32_t ready;  // == the launch's epoch once the item is written
+};
+
+struct HandoffQueue {
+    Handoff *items = nullptr;       // nullptr: donation off
+    unsigned long long cap = 0;
+    unsigned long long *ctr = nullptr;  // [0] head, [1] tail, [2] idle warps, [3] exited warps
+    uint32_t epoch = 0;
+    uint32_t v_cnt = 0;  // items naming a vertex >= v_cnt are rejected
+};
+
+// Smallest ranges worth handing off: leaf candidates (lane-parallel) and
+// intermediate-level candidates (each a whole subtree).
+#ifndef GI_LEAF_HANDOFF_MIN
+#define GI_LEAF_HANDOFF_MIN 64
+#endif
+constexpr int kLeafHandoffMin = GI_LEAF_HANDOFF_MIN;
+constexpr int kMidHandoffMin = 4;
 
 __device__ __forceinline__ unsigned long long globaltimer() {
     unsigned long long t;
@@ -244,7 +275,10 @@ __device__ __forceinline__ int lane_cost(int x, int y) {
 }
 
 // A leaf candidate costlier than this for one lane goes to the whole warp.
-constexpr int kLaneBudget = 2048;
+#ifndef GI_LANE_BUDGET
+#define GI_LANE_BUDGET 2048
+#endif
+constexpr int kLaneBudget = GI_LANE_BUDGET;
 
 // How many of emb[0, d) occur in s[0, n), warp-cooperative.
 __device__ __forceinline__ int warp_count_embedded(const uint32_t *s, int n, const WarpState &w, int d, int lane) {
@@ -312,6 +346,28 @@ struct Ctx {
     unsigned long long t_start = 0;
     unsigned long long hard_ns = 0;  // > 0: give up the current work item past this much time
     bool aborted = false;
+    HandoffQueue hq{};
+
+    // Offers [lo, hi) of depth d's loop to an idle warp (warp-uniform);
+    // true when it was queued and is no longer this warp's to do.
+    __device__ __forceinline__ bool donate(int d, int lo, int hi) {
+        int ok = 0;
+        if (d < 2 || d >= P.stop || lo < 0 || hi <= lo) return false;  // not a handoff range
+        if (lane == 0 && *(volatile unsigned long long *)&hq.ctr[2] > 0) {
+            const unsigned long long slot = atomicAdd(&hq.ctr[1], 1ull);
+            if (slot < hq.cap) {
+                Handoff &h = hq.items[slot];
+                for (int u = 0; u < d; ++u) h.emb[u] = w.emb[u];
+                h.depth = d;
+                h.lo = lo;
+                h.hi = hi;
+                __threadfence();
+                *(volatile uint32_t *)&h.ready = hq.epoch;
+                ok = 1;
+            }
+        }
+        return __shfl_sync(kFull, ok, 0) != 0;
+    }
 
     // Warp-uniform: true once the hard time limit has passed (lane 0's
     // clock decides for the warp).
@@ -345,10 +401,10 @@ struct Ctx {
                     uint32_t *out = slot_base + static_cast<int64_t>(P.slot[p]) * slot_stride;
                     size = warp_intersect(fs, fn, nb, deg, out, lane);
                     if (lane == 0) w.set_ptr[p] = out;
-                    if (kBytesOn && lane == 0) bytes += 4ull * (fn + deg + size);
+                    if (kBytesOn && account && lane == 0) bytes += 4ull * (fn + deg + size);
                 } else {
                     size = warp_intersect(fs, fn, nb, deg, nullptr, lane);
-                    if (kBytesOn && lane == 0) bytes += 4ull * (fn + deg);
+                    if (kBytesOn && account && lane == 0) bytes += 4ull * (fn + deg);
                 }
             }
             if (lane == 0) w.set_size[p] = size;
@@ -545,6 +601,10 @@ struct Ctx {
         unsigned long long acc = 0;
         for (int base = i0; base < i1; base += 32) {
             if (out_of_time()) break;
+            if (hq.items && i1 - base >= 2 * kLeafHandoffMin) {
+                const int mid = base + ((i1 - base) / 2 + 31) / 32 * 32;
+                if (mid < i1 && donate(D, mid, i1)) i1 = mid;
+            }
             const int i = base + lane;
             uint32_t v = 0;
             bool heavy = false;
@@ -574,39 +634,51 @@ struct Ctx {
 
     // The DFS below the first two positions for depth-2 candidates [lo, hi);
     // returns the subtask's sum (warp-uniform).
-    __device__ unsigned long long dfs(int lo, int hi) {
+    __device__ unsigned long long dfs(int lo, int hi) { return dfs_from(2, lo, hi); }
+
+    // The DFS from depth `base` (>= 2, emb[0, base) and their prefix sets in
+    // place) over loop indices [lo, hi) of that depth.
+    __device__ unsigned long long dfs_from(int base, int lo, int hi) {
         const int stop = P.stop;
         const int leaf = P.leaf_depth;
         unsigned long long acc = 0;
         if (lane == 0) {
-            w.cursor[2] = lo;
-            w.end[2] = hi;
-            w.minv[2] = min_vertex(2);
+            w.cursor[base] = lo;
+            w.end[base] = hi;
+            w.minv[base] = min_vertex(base);
         }
         __syncwarp();
-        if (leaf == 2) return leaf_level(2, lo, hi);
-        int d = 2;
+        if (leaf == base) return leaf_level(base, lo, hi);
+        int d = base;
         while (true) {
             if (out_of_time()) break;
             if (d == stop) {
                 acc += P.iep_k > 0 ? iep_tail(d) : last_level(d);
                 --d;
-                if (d < 2) break;
+                if (d < base) break;
                 continue;
             }
             if (d == leaf) {
                 acc += leaf_level(d, 0, 0x7fffffff);
                 --d;
-                if (d < 2) break;
+                if (d < base) break;
                 continue;
             }
             const int ls = P.loop_set[d];
             const uint32_t *s = w.set_ptr[ls];
-            const int ns = min(w.set_size[ls], w.end[d]);
+            int ns = min(w.set_size[ls], w.end[d]);
             const uint32_t bound = w.minv[d];
             int i = w.cursor[d];
             bool descended = false;
             while (i < ns) {
+                if (hq.items && ns - i >= 2 * kMidHandoffMin) {
+                    const int mid = i + (ns - i + 1) / 2;
+                    if (donate(d, mid, ns)) {
+                        ns = mid;
+                        if (lane == 0) w.end[d] = mid;
+                        __syncwarp();
+                    }
+                }
                 const uint32_t v = s[i++];
                 if (v >= bound) {
                     i = ns;
@@ -634,9 +706,32 @@ struct Ctx {
             }
             if (descended) continue;
             --d;
-            if (d < 2) break;
+            if (d < base) break;
         }
         return acc;
+    }
+
+    // Runs a handed-off item: rebuilds the prefix sets of emb[0, depth) (no
+    // byte accounting: the donor already counted them) and the range.
+    // The item is read through L2 (ld.global.cg): it was written by another
+    // SM after this launch began.
+    // Returns false (and counts nothing) for an item that fails its checks.
+    __device__ bool run_handoff(const Handoff *h, unsigned long long &out) {
+        const int D = __ldcg(&h->depth);
+        const int lo = __ldcg(&h->lo), hi = __ldcg(&h->hi);
+        out = 0;
+        if (D < 2 || D >= P.stop || lo < 0 || hi < lo) return false;
+        const uint32_t x = lane < D ? __ldcg(&h->emb[lane]) : 0u;
+        if (__any_sync(kFull, lane < D && x >= hq.v_cnt)) return false;
+        if (lane < D) w.emb[lane] = x;
+        __syncwarp();
+        // Depth 0 is built unconditionally, as the chunk path does; deeper
+        // chains passed their break-size prune when the donor built them.
+        build_chain(0, w.emb[0], false);
+        for (int j = 1; j < D; ++j)
+            if (!build_chain(j, w.emb[j], false)) return true;
+        out = dfs_from(D, lo, hi);
+        return true;
     }
 };
 

@@ -77,6 +77,7 @@ void graph_free(gi_graph *g) {
     cudaFree(g->d_counters);
     cudaFree(g->d_offsets);
     cudaFree(g->d_scan_tmp);
+    cudaFree(g->d_handoff);
     cudaFree(g->d_bitmap);
     cudaFree(g->d_bitmap_off);
     cudaSetDevice(prev);

@@ -91,6 +91,10 @@ struct gi_graph {
     int64_t *d_offsets = nullptr;
     void *d_scan_tmp = nullptr;
     size_t scan_tmp_bytes = 0;
+    // Work-donation queue of the counting kernel (kept between counts, its
+    // ready flags tagged with a per-launch epoch so it never needs clearing).
+    void *d_handoff = nullptr;
+    uint32_t handoff_epoch = 0;
     // Lazily built derived graphs (clique orientations).
     gi_graph *oriented[2] = {nullptr, nullptr};
     // Per-vertex adjacency bitmaps of a degree-oriented DAG (kclique.cu),

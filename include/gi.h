@@ -199,6 +199,10 @@ typedef struct gi_stats {
     int64_t chunks_total;    /* out: work chunks in the shard */
     double prep_ms;          /* out: device time of the work-split pre-pass (once per count,
                                 not included in kernel_ms) */
+    int64_t sample_chunks;   /* in (gi_count_shard only): > 0 = count only the first
+                                sample_chunks chunks of the shard in the same fixed pseudo-random
+                                order, all of them to completion: a uniform sample whose chunks,
+                                and hence raw_sum, are the same on every call */
 } gi_stats;
 
 /* Replaces gpu_pattern_matching<<<...>>> + the D2H of dev_sum + the

@@ -257,3 +257,28 @@ def test_kclique_bitmaps_match_the_dfs_path_and_closed_forms(oracle):
         dg = gi.Graph.from_csr(*(lambda c: (c.vertex, c.edge))(_complete(n)))
         for k in ks:
             assert gi.clique_count(dg, k, 1).count == comb(n, k) % (1 << 64), (n, k)
+
+
+def test_fixed_samples_repeat_exactly_and_grow_to_the_whole_shard(golden_graphs, dev_graphs):
+    """gi_stats.sample_chunks: the first M chunks of the shard's pseudo-random
+    order, each counted to completion — the same raw sum on every call, and,
+    when M covers every shard, shards that add up to the whole count."""
+    g, dg = golden_graphs["rmat_s10_ef12"], dev_graphs["rmat_s10_ef12"]
+    s = gi.Schedule_IEP(gi.Pattern(5, "0101110101010101010011000"), g.v_cnt, g.e_cnt, 0)
+
+    def run(shard, m):
+        st = N.Stats()
+        st.sample_chunks = m
+        raw = C.c_uint64()
+        N.check(gi.lib().gi_count_shard(dg.handle, s.handle, shard, 3, None, C.byref(raw), C.byref(st)), "shard")
+        return raw.value, st
+
+    a, sa = run(1, 7)
+    b, sb = run(1, 7)
+    assert a == b and sa.chunks_done == sb.chunks_done == 7 < sa.chunks_total
+    total = 0
+    for shard in range(3):
+        raw, st = run(shard, 1 << 40)
+        assert st.chunks_done == st.chunks_total
+        total = (total + raw) % (1 << 64)
+    assert total == gi.pattern_matching(dg, s).raw_sum
