@@ -101,6 +101,12 @@ static int build_dev_plan(const Schedule_IEP &s, DevPlan &d) {
         for (int j = 0; j < n; ++j)
             if (i != j && !d.adj[i * n + j]) anti_edge = true;
     d.leaf_depth = (d.stop - 1 >= 2 && !(d.vertex_induced && anti_edge)) ? d.stop - 1 : -1;
+    // Lane-versus-warp split of leaf candidates, measured on the B200 (R-MAT
+    // scales 14-17): plans with an IEP tail evaluate several intersections per
+    // candidate and run best when only cheap candidates stay on one lane
+    // (house 11 %, prism 5 %, 6-cycle + chord 4 % faster at 256 than at 2048);
+    // plans without one (cliques) prefer the lanes (5-clique 36 % faster at 2048).
+    d.lane_budget = d.iep_k > 0 ? 256 : 2048;
     for (int p = 0; p < GI_MAX_PREFIX; ++p) d.pdepth[p] = p < tp ? s.get_prefix_data(p).back() : -1;
     // Splitting of the depth-2 loop: its set's members are a subset of {0, 1}.
     d.loop2_kind = -1;

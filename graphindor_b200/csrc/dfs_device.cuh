@@ -274,11 +274,13 @@ __device__ __forceinline__ int lane_cost(int x, int y) {
     return lo * (33 - __clz(hi / lo + 1));
 }
 
-// A leaf candidate costlier than this for one lane goes to the whole warp.
-#ifndef GI_LANE_BUDGET
-#define GI_LANE_BUDGET 2048
+// A leaf candidate costlier than DevPlan::lane_budget for one lane goes to the
+// whole warp; GI_LANE_BUDGET (experiments) overrides every plan's value.
+#ifdef GI_LANE_BUDGET
+constexpr int kLaneBudgetOverride = GI_LANE_BUDGET;
+#else
+constexpr int kLaneBudgetOverride = -1;
 #endif
-constexpr int kLaneBudget = GI_LANE_BUDGET;
 
 // How many of emb[0, d) occur in s[0, n), warp-cooperative.
 __device__ __forceinline__ int warp_count_embedded(const uint32_t *s, int n, const WarpState &w, int d, int lane) {
@@ -582,8 +584,8 @@ struct Ctx {
 
     // Leaf-parent depth D: every candidate of the loop set in [i0, i1) below
     // the restriction bound, one per lane; a candidate whose intersections
-    // would keep one lane busy for more than kLaneBudget steps (hub against
-    // hub) is handed to the whole warp instead.  Returns the warp's sum.
+    // would keep one lane busy for more than the plan's lane budget (hub
+    // against hub) is handed to the whole warp instead.  Returns the warp's sum.
     __device__ unsigned long long leaf_level(int D, int i0, int i1) {
         const int ls = P.loop_set[D];
         const uint32_t *s = w.set_ptr[ls];
@@ -617,7 +619,7 @@ struct Ctx {
                     int cost = 0;
                     for (int p = P.last[D]; p != -1; p = P.next[p])
                         if (P.father[p] >= 0) cost += lane_cost(w.set_size[P.father[p]], dv);
-                    heavy = cost > kLaneBudget;
+                    heavy = cost > (kLaneBudgetOverride >= 0 ? kLaneBudgetOverride : P.lane_budget);
                     if (!heavy) acc += leaf_eval<false>(D, v);
                 }
             }

@@ -37,6 +37,7 @@ struct DevPlan {
     int32_t vertex_induced;
     int32_t stop;               // depth closed in form: n - iep_k with IEP, else n - 1
     int32_t leaf_depth;         // stop - 1 when its candidates run one per lane, else -1
+    int32_t lane_budget;        // leaf candidates costlier than this for one lane go to the warp
     int32_t loop2_kind;         // bound of the depth-2 loop set: 0 d(v0), 1 d(v1), 2 min, -1 none
     int32_t pdepth[GI_MAX_PREFIX];  // last member (position) of each prefix
     int32_t father[GI_MAX_PREFIX];
