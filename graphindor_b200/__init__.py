@@ -128,6 +128,27 @@ class Schedule_IEP:
             out[key] = list(buf[: n_raw.value])
         return out
 
+    @classmethod
+    def learned(cls, pattern: Pattern, graph: "Graph", enable_iep: bool = True,
+                model_path: Optional[str] = None) -> "Schedule_IEP":
+        """The valid candidate schedule with the smallest device time the
+        learned cost model predicts on `graph` (exact counts).  Loads the
+        package's trained model on first use unless model_path is given."""
+        L = lib()
+        load_cost_model(model_path)
+        feats = (C.c_float * N.GI_GRAPH_FEATURES)()
+        check(L.gi_graph_features(graph.handle, feats, N.GI_GRAPH_FEATURES), "gi_graph_features")
+        h = C.c_void_p()
+        pred = C.c_double()
+        check(L.gi_plan_create_learned(pattern.size, pattern.adj_string.encode(), graph.v_cnt, graph.e_cnt,
+                                       graph.tri_cnt, feats, int(enable_iep), C.byref(h), C.byref(pred)),
+              "gi_plan_create_learned")
+        obj = cls.__new__(cls)
+        obj._h = h
+        obj.pattern = pattern
+        obj.predicted_ms = pred.value
+        return obj
+
     @staticmethod
     def candidates(pattern: Pattern, v_cnt: int, e_cnt: int, tri_cnt: int, enable_iep: bool = True):
         """(order, restricts, analytic cost, exact divisor or 0 if the
@@ -150,6 +171,20 @@ class Schedule_IEP:
             r = [(rs[(i * N.GI_MAX_PREFIX + j) * 2], rs[(i * N.GI_MAX_PREFIX + j) * 2 + 1]) for j in range(nr[i])]
             out.append((list(orders[i * n:(i + 1) * n]), r, costs[i], divs[i]))
         return out
+
+
+COST_MODEL_PATH = __import__("pathlib").Path(__file__).resolve().parent / "schedule_cost" / "weights.bin"
+_cost_model_loaded: Optional[str] = None
+
+
+def load_cost_model(path: Optional[str] = None) -> None:
+    """Loads the learned schedule cost model (default: the trained weights
+    shipped in the package) once per process."""
+    global _cost_model_loaded
+    p = str(path or COST_MODEL_PATH)
+    if _cost_model_loaded != p:
+        check(lib().gi_cost_model_load(p.encode()), "gi_cost_model_load")
+        _cost_model_loaded = p
 
 
 @dataclass

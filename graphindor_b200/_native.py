@@ -81,6 +81,7 @@ class LabeledGraphInfo(C.Structure):
 
 
 GI_FSM_MAX_PATTERNS = 64
+GI_GRAPH_FEATURES = 19
 
 
 class FsmPattern(C.Structure):
@@ -138,6 +139,11 @@ _SIGS = {
                          C.POINTER(FsmStats)]),
     "gi_fsm_plan": (C.c_int, [C.c_int, C.c_int32, C.c_int64, C.c_int64, C.POINTER(FsmPattern), C.c_int,
                               C.POINTER(C.c_int)]),
+    "gi_cost_model_load": (C.c_int, [C.c_char_p]),
+    "gi_graph_features": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
+    "gi_graph_features_host": (C.c_int, [C.c_void_p, C.c_int32, C.c_int64, C.c_void_p, C.c_int]),
+    "gi_plan_create_learned": (C.c_int, [C.c_int, C.c_char_p, C.c_int32, C.c_int64, C.c_int64, C.c_void_p, C.c_int,
+                                         C.POINTER(C.c_void_p), C.POINTER(C.c_double)]),
 }
 
 _lib = None

@@ -58,6 +58,8 @@ __global__ void build_edge_from_kernel(const int64_t *__restrict__ vertex, const
 
 }  // namespace
 
+void cost_model_graph_features(const int64_t *vertex, int32_t v_cnt, int64_t tri_cnt, float *out);
+
 int cuda_fail(cudaError_t e, const char *what) {
     char buf[256];
     std::snprintf(buf, sizeof(buf), "%s: %s", what, cudaGetErrorString(e));
@@ -120,6 +122,7 @@ int graph_create_impl(const int64_t *vertex, const int32_t *edge, int32_t v_cnt,
     g->e_cnt = e_cnt;
     g->tri_cnt = tri_cnt;
     degree_stats(vertex, v_cnt, g->max_degree, g->max_isect);
+    cost_model_graph_features(vertex, v_cnt, tri_cnt, g->graph_features);
     cudaError_t e;
     const size_t vb = sizeof(int64_t) * (static_cast<size_t>(v_cnt) + 1);
     const size_t eb = sizeof(int32_t) * static_cast<size_t>(e_cnt > 0 ? e_cnt : 1);

@@ -92,6 +92,10 @@ struct gi_graph {
     int64_t *d_offsets = nullptr;
     void *d_scan_tmp = nullptr;
     size_t scan_tmp_bytes = 0;
+    // Features of the learned schedule cost model (schedule_cost.cpp):
+    // log10 v_cnt, edges and triangles, then the share of vertices per
+    // power-of-two degree bin.
+    float graph_features[3 + 16] = {};
     // Work-donation queue of the counting kernel (kept between counts, its
     // ready flags tagged with a per-launch epoch so it never needs clearing).
     void *d_handoff = nullptr;

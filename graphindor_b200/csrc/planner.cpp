@@ -979,7 +979,8 @@ std::vector<Schedule_IEP::Candidate> Schedule_IEP::enumerate_candidates(const Pa
             for (const auto &p : filter_implied(pairs))
                 if (p.second < n - s.in_exclusion_optimize_num) applied.push_back(p);
             const int div = restriction_multiplicity(s.adj_mat.data(), n, applied);
-            out.push_back({vec, pairs, s.new_estimate_schedule_restrict(pairs, v_cnt, e_cnt, tri_cnt), div});
+            out.push_back({vec, pairs, s.new_estimate_schedule_restrict(pairs, v_cnt, e_cnt, tri_cnt), div,
+                           s.in_exclusion_optimize_num});
         }
     }
     return out;

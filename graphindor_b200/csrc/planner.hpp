@@ -124,6 +124,7 @@ public:
         std::vector<std::pair<int, int>> restricts;
         double model_cost;
         int divisor;  // exact count divisor, 0 when the restriction set is not valid
+        int iep_k = 0;  // in_exclusion_optimize_num of the order
     };
     // The lowest-cost candidate whose restriction set is valid (ties: first
     // in enumeration order).  Returns false if there is none.

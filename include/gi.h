@@ -265,6 +265,26 @@ int gi_motif_num(int k);
 int gi_motif_patterns(int k, char *adj_out, int cap);
 int gi_motif_count(const gi_graph *g, int k, gi_stream stream, uint64_t *out_counts, int cap, gi_stats *stats);
 
+/* ------------------------------------------- learned schedule cost model */
+
+/* No reference counterpart: the reference picks a schedule with its analytic
+ * model only (src/schedule_IEP.cpp:307-382).  A small MLP trained on
+ * engine-measured device times (graphindor_b200/schedule_cost/train.py) ranks
+ * the valid candidate schedules (order + restriction set) of a pattern for a
+ * graph described by GI_GRAPH_FEATURES floats. */
+#define GI_GRAPH_FEATURES 19
+/* Loads the model file written by train.py (process-wide; replaces any
+ * loaded model). */
+int gi_cost_model_load(const char *path);
+/* The graph features of a graph handle, or of host CSR offsets. */
+int gi_graph_features(const gi_graph *g, float *out, int cap);
+int gi_graph_features_host(const int64_t *vertex, int32_t v_cnt, int64_t tri_cnt, float *out, int cap);
+/* The valid candidate with the smallest predicted time, as
+ * gi_plan_create_explicit builds it (exact counts).  predicted_ms (optional)
+ * receives the model's prediction. */
+int gi_plan_create_learned(int n, const char *adj, int32_t v_cnt, int64_t e_cnt, int64_t tri_cnt,
+                           const float *graph_features, int enable_iep, gi_plan **out, double *predicted_ms);
+
 /* --------------------------------------------------- labeled graphs + FSM */
 
 /* Replaces DataLoader::load_labeled_data (reference src/dataloader.cpp:

@@ -282,3 +282,16 @@ def test_fixed_samples_repeat_exactly_and_grow_to_the_whole_shard(golden_graphs,
         assert st.chunks_done == st.chunks_total
         total = (total + raw) % (1 << 64)
     assert total == gi.pattern_matching(dg, s).raw_sum
+
+
+def test_learned_schedules_count_exactly(golden_graphs, dev_graphs, oracle):
+    """The learned cost model picks among valid candidates only, so its plans
+    count exactly: equal to the validated analytic plan (model 2)."""
+    g, dg = golden_graphs["rmat_s9_ef8"], dev_graphs["rmat_s9_ef8"]
+    for n, adj in [(4, "0110100110010110"), (5, "0101110101010101010011000"),
+                   (6, "011100101010110001100011010101001110"), (6, "010101101000010100101010000101100010")]:
+        p = gi.Pattern(n, adj)
+        learned = gi.Schedule_IEP.learned(p, dg)
+        assert learned.export()["exact"] == 1
+        exact = gi.Schedule_IEP(p, g.v_cnt, g.e_cnt, 0, model=2)
+        assert gi.pattern_matching(dg, learned).count == gi.pattern_matching(dg, exact).count, adj

@@ -1,0 +1,59 @@
+"""The learned schedule cost model on the CPU: the engine's features and MLP
+forward pass (csrc/schedule_cost.cpp) agree with the Python definitions used
+for training (graphindor_b200/schedule_cost), and a learned plan is one of
+the pattern's valid candidates, so its count is exact."""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import graphindor_b200 as gi
+from graphindor_b200 import _native as N
+from graphindor_b200 import gen
+from graphindor_b200.schedule_cost.features import DIM, graph_features, plan_features
+from graphindor_b200.schedule_cost.train import HIDDEN, MLP, save
+
+
+def test_graph_features_match(native):
+    for g, tri in ((gen.rmat(12, 8.0, 3), 12345), (gen.erdos_renyi(3000, 20000, 4), 0)):
+        f = (C.c_float * N.GI_GRAPH_FEATURES)()
+        N.check(gi.lib().gi_graph_features_host(g.vertex.ctypes.data, g.v_cnt, tri, f, N.GI_GRAPH_FEATURES), "f")
+        assert np.allclose(np.array(f[:]), graph_features(g.vertex, tri), atol=1e-6)
+
+
+@pytest.mark.parametrize("seed", [1, 2])
+def test_learned_choice_is_the_python_argmin(tmp_path, native, seed):
+    mlp = MLP(DIM, HIDDEN, seed)
+    rng = np.random.default_rng(seed)
+    mu = rng.standard_normal(DIM).astype(np.float32) * 0.1
+    sd = (1.0 + rng.random(DIM)).astype(np.float32)
+    path = tmp_path / "w.bin"
+    save(str(path), mlp, mu, sd)
+    gi.load_cost_model(str(path))
+    g = gen.rmat(11, 8.0, 5)
+    gf = graph_features(g.vertex, 777)
+    feats = (C.c_float * N.GI_GRAPH_FEATURES)(*gf.tolist())
+    for n, adj in [(5, "0101110101010101010011000"), (6, "011100101010110001100011010101001110"),
+                   (4, "0110100110010110")]:
+        p = gi.Pattern(n, adj)
+        cands = [c for c in gi.Schedule_IEP.candidates(p, g.v_cnt, g.e_cnt, 777) if c[3] > 0]
+        k = gi.Schedule_IEP(p, order=cands[0][0], restricts=cands[0][1]).export()["in_exclusion_optimize_num"]
+        X = np.stack([np.concatenate([plan_features(n, adj, o, r, cost, k), gf]) for o, r, cost, _ in cands])
+        pred, _ = mlp.forward((X - mu) / sd)
+        want = cands[int(np.argmin(pred))]
+        h = C.c_void_p()
+        ms = C.c_double()
+        N.check(gi.lib().gi_plan_create_learned(n, adj.encode(), g.v_cnt, g.e_cnt, 777, feats, 1, C.byref(h),
+                                                C.byref(ms)), "learned")
+        s = gi.Schedule_IEP.__new__(gi.Schedule_IEP)
+        s._h, s.pattern = h, p
+        e = s.export()
+        assert e["order"] == list(want[0]) and e["exact"] == 1
+        assert ms.value == pytest.approx(10.0 ** float(pred.min()), rel=1e-3)
+    gi.load_cost_model()  # back to the shipped model (if present) for later tests
+
+
+def test_missing_model_file_is_an_error(native):
+    assert gi.lib().gi_cost_model_load(b"/nonexistent/w.bin") == N.GI_EIO
