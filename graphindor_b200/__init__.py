@@ -18,7 +18,7 @@ from ._native import GIError, check, lib
 
 __all__ = ["Pattern", "Schedule_IEP", "Graph", "pattern_matching", "clique_count", "motif_counting",
            "motif_patterns", "GIError", "lib", "write_g", "read_g", "LabeledGraph", "fsm", "fsm_plan",
-           "FsmResult", "PATENTS_TRI_CNT", "YOUTUBE_TRI_CNT"]
+           "FsmResult", "PATENTS_TRI_CNT", "YOUTUBE_TRI_CNT", "Batch", "load_cost_model"]
 
 
 class Pattern:
@@ -423,3 +423,35 @@ def fsm_plan(max_edge: int, v_cnt: int, e_cnt: int, tri_cnt: int = YOUTUBE_TRI_C
     check(lib().gi_fsm_plan(max_edge, v_cnt, e_cnt, tri_cnt, pats, N.GI_FSM_MAX_PATTERNS, C.byref(cnt)),
           "gi_fsm_plan")
     return [_fsm_pattern(pats[i]) for i in range(min(cnt.value, N.GI_FSM_MAX_PATTERNS))]
+
+
+# ------------------------------------------------------------------ batches
+
+class Batch:
+    """Many (graph, plan) jobs counted in one persistent launch, captured in a
+    CUDA graph on the first run and replayed afterwards."""
+
+    def __init__(self, jobs: Sequence[tuple["Graph", "Schedule_IEP"]]):
+        self._keep = list(jobs)  # the handles must outlive the batch
+        n = len(self._keep)
+        graphs = (C.c_void_p * n)(*[g.handle for g, _ in self._keep])
+        plans = (C.c_void_p * n)(*[p.handle for _, p in self._keep])
+        h = C.c_void_p()
+        check(lib().gi_batch_create(graphs, plans, n, C.byref(h)), "gi_batch_create")
+        self._h = h
+        self.n_jobs = n
+
+    def run(self, stream: int = 0):
+        """(counts, per-job device ms from launch start to job end, kernel ms)."""
+        counts = (C.c_uint64 * self.n_jobs)()
+        ms = (C.c_double * self.n_jobs)()
+        st = N.Stats()
+        check(lib().gi_batch_run(self._h, C.c_void_p(stream) if stream else None, counts, ms, C.byref(st)),
+              "gi_batch_run")
+        return [int(x) for x in counts], [float(x) for x in ms], st.kernel_ms
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            lib().gi_batch_destroy(h)
+            self._h = None

@@ -140,6 +140,9 @@ _SIGS = {
     "gi_fsm_plan": (C.c_int, [C.c_int, C.c_int32, C.c_int64, C.c_int64, C.POINTER(FsmPattern), C.c_int,
                               C.POINTER(C.c_int)]),
     "gi_cost_model_load": (C.c_int, [C.c_char_p]),
+    "gi_batch_create": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.POINTER(C.c_void_p)]),
+    "gi_batch_run": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(Stats)]),
+    "gi_batch_destroy": (C.c_int, [C.c_void_p]),
     "gi_graph_features": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
     "gi_graph_features_host": (C.c_int, [C.c_void_p, C.c_int32, C.c_int64, C.c_void_p, C.c_int]),
     "gi_plan_create_learned": (C.c_int, [C.c_int, C.c_char_p, C.c_int32, C.c_int64, C.c_int64, C.c_void_p, C.c_int,

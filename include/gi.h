@@ -265,6 +265,22 @@ int gi_motif_num(int k);
 int gi_motif_patterns(int k, char *adj_out, int cap);
 int gi_motif_count(const gi_graph *g, int k, gi_stream stream, uint64_t *out_counts, int cap, gi_stats *stats);
 
+/* -------------------------------------------------------- batched counts */
+
+/* No single reference counterpart: the reference launches one kernel per
+ * (pattern, graph) (gpu/gpu_graph.cu:22-51; gpu/gpu_mc.cu:93-112 loops over
+ * patterns).  A batch fixes n_jobs (graph, plan) pairs, job i =
+ * (graphs[i], plans[i]), all graphs on one device; the handles must outlive
+ * the batch.  gi_batch_run counts every job in one persistent launch (the
+ * first run captures it in a CUDA graph, later runs replay it) and writes
+ * counts[i] (gpu_graph semantics, as gi_count) and, optionally, job_ms[i]:
+ * device time from the launch's first warp to the end of job i's last work
+ * item.  Runs of one batch must not overlap. */
+typedef struct gi_batch gi_batch;
+int gi_batch_create(gi_graph *const *graphs, const gi_plan *const *plans, int n_jobs, gi_batch **out);
+int gi_batch_run(gi_batch *b, gi_stream stream, uint64_t *counts, double *job_ms, gi_stats *stats);
+int gi_batch_destroy(gi_batch *b);
+
 /* ------------------------------------------- learned schedule cost model */
 
 /* No reference counterpart: the reference picks a schedule with its analytic

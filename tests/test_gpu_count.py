@@ -295,3 +295,26 @@ def test_learned_schedules_count_exactly(golden_graphs, dev_graphs, oracle):
         assert learned.export()["exact"] == 1
         exact = gi.Schedule_IEP(p, g.v_cnt, g.e_cnt, 0, model=2)
         assert gi.pattern_matching(dg, learned).count == gi.pattern_matching(dg, exact).count, adj
+
+
+def test_batch_counts_match_single_counts(golden_graphs, dev_graphs):
+    """One launch for (pattern, graph) jobs across four graphs, a graph with
+    no edges among them; the first run captures the CUDA graph, the second
+    replays it."""
+    empty = gi.Graph.from_csr(np.array([0, 0, 0], dtype=np.int64), np.zeros(0, dtype=np.int32))
+    pats = [(3, "011101110"), (4, "0111101111001100"), (4, "0110100110010110"), (5, "0101110101010101010011000"),
+            (5, "0111110111110111110111110")]
+    jobs, want = [], []
+    for name, g in golden_graphs.items():
+        for n, adj in pats:
+            s = gi.Schedule_IEP(gi.Pattern(n, adj), g.v_cnt, g.e_cnt, 0)
+            jobs.append((dev_graphs[name], s))
+            want.append(gi.pattern_matching(dev_graphs[name], s).count)
+    s0 = gi.Schedule_IEP(gi.Pattern(4, "0110100110010110"), 2, 1, 0, model=0)
+    jobs.insert(3, (empty, s0))
+    want.insert(3, 0)
+    b = gi.Batch(jobs)
+    for _ in range(2):
+        counts, ms, kernel_ms = b.run()
+        assert counts == want
+        assert kernel_ms > 0 and all(m >= 0 for m in ms) and ms[3] == 0.0
