@@ -131,6 +131,31 @@ def save(path: str, mlp: MLP, mu: np.ndarray, sd: np.ndarray) -> None:
             f.write(np.ascontiguousarray(a, dtype="<f4").tobytes())
 
 
+def load(path: str):
+    """(MLP, feature means, feature scales) from a file written by save()."""
+    raw = open(path, "rb").read()
+    assert raw[:8] == b"GIMLP1\0\0", "not a schedule cost model file"
+    d_in, hidden = struct.unpack_from("<ii", raw, 8)
+    a = np.frombuffer(raw, dtype="<f4", offset=16)
+    sizes = [d_in, d_in, hidden * d_in, hidden, hidden * hidden, hidden, hidden, 1]
+    parts, o = [], 0
+    for n in sizes:
+        parts.append(a[o:o + n].copy())
+        o += n
+    m = MLP(d_in, hidden)
+    m.W1, m.b1 = parts[2].reshape(hidden, d_in), parts[3]
+    m.W2, m.b2 = parts[4].reshape(hidden, hidden), parts[5]
+    m.w3, m.b3 = parts[6], np.float32(parts[7][0])
+    return m, parts[0], parts[1]
+
+
+def split(keys, seed: int = 0):
+    """The seeded 70/30 split by pattern used for training."""
+    pats = sorted({k[1] for k in keys})
+    random.Random(seed).shuffle(pats)
+    return set(pats[: int(round(0.3 * len(pats)))])
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("runs")
@@ -140,9 +165,7 @@ def main():
     a = ap.parse_args()
     X, y, keys, censored, runs = load_rows(a.runs)
     assert X.shape[1] == DIM
-    pats = sorted({k[1] for k in keys})
-    random.Random(a.seed).shuffle(pats)
-    test_p = set(pats[: int(round(0.3 * len(pats)))])
+    test_p = split(keys, a.seed)
     train = np.asarray([k[1] not in test_p for k in keys])
     mu = X[train].mean(0)
     sd = X[train].std(0) + 1e-6

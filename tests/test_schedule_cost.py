@@ -57,3 +57,21 @@ def test_learned_choice_is_the_python_argmin(tmp_path, native, seed):
 
 def test_missing_model_file_is_an_error(native):
     assert gi.lib().gi_cost_model_load(b"/nonexistent/w.bin") == N.GI_EIO
+
+
+def test_shipped_model_against_the_analytic_choice_on_held_out_patterns():
+    """What the trained network gains over the analytic model on the patterns
+    it was not trained on (the committed B200 timings, seeded split): its
+    picks must not be slower in total than the analytic model's."""
+    from pathlib import Path
+    from graphindor_b200.schedule_cost import train
+    here = Path(gi.__file__).resolve().parent / "schedule_cost"
+    X, y, keys, censored, runs = train.load_rows(str(here / "runs_b200.json"))
+    mlp, mu, sd = train.load(str(here / "weights.bin"))
+    pred, _ = mlp.forward((X - mu) / sd)
+    test_p = train.split(keys, 0)
+    rep = train.selection_report(keys, 10.0 ** y, pred, [r["model_cost"] for r in runs["rows"]],
+                                 {k for k in keys if k[1] in test_p})
+    assert rep["cases"] >= 20
+    assert rep["learned_total_ms"] <= rep["analytic_total_ms"]
+    assert rep["learned_regret_median"] <= rep["analytic_regret_median"]
