@@ -141,6 +141,10 @@ _SIGS = {
                               C.POINTER(C.c_int)]),
     "gi_cost_model_load": (C.c_int, [C.c_char_p]),
     "gi_batch_create": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.POINTER(C.c_void_p)]),
+    "gi_mlp_grad": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p,
+                              C.POINTER(C.c_float)]),
+    "gi_mlp_train": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float,
+                               C.c_float, C.c_uint64, C.c_void_p, C.POINTER(C.c_float)]),
     "gi_batch_run": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(Stats)]),
     "gi_batch_destroy": (C.c_int, [C.c_void_p]),
     "gi_graph_features": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),

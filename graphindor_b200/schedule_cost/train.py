@@ -59,6 +59,30 @@ class MLP:
     def params(self):
         return [self.W1, self.b1, self.W2, self.b2, self.w3]
 
+    def pack(self) -> np.ndarray:
+        """All parameters as one float32 array, in the model file's order."""
+        return np.concatenate([self.W1.ravel(), self.b1, self.W2.ravel(), self.b2, self.w3,
+                               np.asarray([self.b3], np.float32)]).astype(np.float32)
+
+    def unpack(self, p: np.ndarray) -> None:
+        H, I = self.W1.shape
+        o = 0
+        for name, shape in (("W1", (H, I)), ("b1", (H,)), ("W2", (H, H)), ("b2", (H,)), ("w3", (H,))):
+            n = int(np.prod(shape))
+            setattr(self, name, p[o:o + n].reshape(shape).astype(np.float32).copy())
+            o += n
+        self.b3 = np.float32(p[o])
+
+    def grads(self, X, y) -> np.ndarray:
+        """Gradient of the mean squared error over the rows of X, packed like
+        pack() (the host oracle of the GPU kernels)."""
+        pred, (x0, h1, h2) = self.forward(X)
+        g = 2.0 * (pred - y) / len(X)
+        gh2 = np.outer(g, self.w3) * (h2 > 0)
+        gh1 = (gh2 @ self.W2) * (h1 > 0)
+        return np.concatenate([(gh1.T @ x0).ravel(), gh1.sum(0), (gh2.T @ h1).ravel(), gh2.sum(0), h2.T @ g,
+                               [g.sum()]]).astype(np.float32)
+
     def forward(self, X):
         h1 = np.maximum(X @ self.W1.T + self.b1, 0)
         h2 = np.maximum(h1 @ self.W2.T + self.b2, 0)
@@ -96,6 +120,22 @@ class MLP:
                         ps[i] -= step.astype(np.float32)
                     else:
                         self.b3 = np.float32(self.b3 - step)
+
+
+def train_gpu(mlp: MLP, X, y, epochs=400, lr=2e-3, batch=128, wd=1e-4, seed=0) -> float:
+    """Trains `mlp` in place with gi_mlp_train (the engine's kernels);
+    returns the final training loss."""
+    import ctypes as C
+
+    from .. import _native as N
+    X = np.ascontiguousarray(X, dtype=np.float32)
+    y = np.ascontiguousarray(y, dtype=np.float32)
+    p = mlp.pack()
+    loss = C.c_float()
+    N.check(N.lib().gi_mlp_train(X.ctypes.data, y.ctypes.data, len(X), X.shape[1], mlp.W1.shape[0], epochs, batch,
+                                 lr, wd, seed, p.ctypes.data, C.byref(loss)), "gi_mlp_train")
+    mlp.unpack(p)
+    return loss.value
 
 
 def selection_report(keys, y_true_ms, pred, model_cost, test_keys):
@@ -162,6 +202,8 @@ def main():
     ap.add_argument("--out", required=True)
     ap.add_argument("--report")
     ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--device", choices=["host", "gpu"], default="host",
+                    help="gpu: train with the engine's CUDA kernels (gi_mlp_train)")
     a = ap.parse_args()
     X, y, keys, censored, runs = load_rows(a.runs)
     assert X.shape[1] == DIM
@@ -171,7 +213,10 @@ def main():
     sd = X[train].std(0) + 1e-6
     Xn = (X - mu) / sd
     mlp = MLP(DIM, HIDDEN, a.seed)
-    mlp.fit(Xn[train], y[train], seed=a.seed)
+    if a.device == "gpu":
+        train_gpu(mlp, Xn[train], y[train], seed=a.seed)
+    else:
+        mlp.fit(Xn[train], y[train], seed=a.seed)
     pred, _ = mlp.forward(Xn)
     ms = 10.0 ** y
     cost = [r["model_cost"] for r in runs["rows"]]

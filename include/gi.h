@@ -300,6 +300,17 @@ int gi_graph_features_host(const int64_t *vertex, int32_t v_cnt, int64_t tri_cnt
  * receives the model's prediction. */
 int gi_plan_create_learned(int n, const char *adj, int32_t v_cnt, int64_t e_cnt, int64_t tri_cnt,
                            const float *graph_features, int enable_iep, gi_plan **out, double *predicted_ms);
+/* Training kernels of that model (3-layer MLP, fp32, ReLU, mean squared
+ * error, Adam).  params: W1 [hidden x in], b1, W2 [hidden x hidden], b2, w3,
+ * b3, the model file's order.  gi_mlp_grad: the loss gradient over all rows
+ * (rows x in inputs X, targets y) and the loss; gi_mlp_train: `epochs`
+ * passes of minibatches of `batch` rows in a seeded shuffle, weight decay wd
+ * on W1, W2 and w3, params updated in place, loss = the final loss over all
+ * rows. */
+int gi_mlp_grad(const float *X, const float *y, int rows, int in, int hidden, const float *params, float *grad_out,
+                float *loss_out);
+int gi_mlp_train(const float *X, const float *y, int rows, int in, int hidden, int epochs, int batch, float lr,
+                 float wd, uint64_t seed, float *params_inout, float *loss_out);
 
 /* --------------------------------------------------- labeled graphs + FSM */
 

@@ -75,3 +75,39 @@ def test_shipped_model_against_the_analytic_choice_on_held_out_patterns():
     assert rep["cases"] >= 20
     assert rep["learned_total_ms"] <= rep["analytic_total_ms"]
     assert rep["learned_regret_median"] <= rep["analytic_regret_median"]
+
+
+def test_host_gradient_oracle_matches_finite_differences():
+    """The host trainer's gradient (the oracle of the GPU training kernels)
+    against central differences in float64."""
+    from graphindor_b200.schedule_cost.train import MLP as M
+    rng = np.random.default_rng(0)
+    m = M(5, 8, 1)
+    X = rng.standard_normal((7, 5))
+    y = np.arange(7, dtype=np.float64)
+    p = m.pack().astype(np.float64)
+
+    def split64(q):  # float64 views in pack() order
+        out, o = [], 0
+        for shape in ((8, 5), (8,), (8, 8), (8,), (8,)):
+            n = int(np.prod(shape))
+            out.append(q[o:o + n].reshape(shape))
+            o += n
+        return out + [float(q[o])]
+
+    def loss(q):
+        W1, b1, W2, b2, w3, b3 = split64(q)
+        h = np.maximum(np.maximum(X @ W1.T + b1, 0) @ W2.T + b2, 0)
+        return float(np.mean((h @ w3 + b3 - y) ** 2))
+
+    m64 = M(5, 8, 0)
+    m64.W1, m64.b1, m64.W2, m64.b2, m64.w3, m64.b3 = split64(p)
+    pr, (x0, h1, h2) = m64.forward(X)
+    g = 2.0 * (pr - y) / len(X)
+    gh2 = np.outer(g, m64.w3) * (h2 > 0)
+    gh1 = (gh2 @ m64.W2) * (h1 > 0)
+    grad = np.concatenate([(gh1.T @ x0).ravel(), gh1.sum(0), (gh2.T @ h1).ravel(), gh2.sum(0), h2.T @ g, [g.sum()]])
+    eye = np.eye(len(p))
+    num = np.array([(loss(p + 1e-6 * eye[i]) - loss(p - 1e-6 * eye[i])) / 2e-6 for i in range(len(p))])
+    assert np.max(np.abs(num - grad)) <= 1e-6 * np.max(np.abs(grad))
+    assert np.allclose(m64.grads(X, y), grad, rtol=1e-5, atol=1e-6)
