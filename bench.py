@@ -312,7 +312,7 @@ def plan_descs(plans):
 
 
 def cpu_job(g, descs, divisors, threads, target_s):
-    """The reference CPU path (oracle) on every s_p-th start vertex per
+    """The reference CPU path (oracle) on every s_p-th directed edge per
     pattern, s_p the power of 4 whose slice takes about target_s; returns
     (whole-job embeddings/s, sample text)."""
     sys.path.insert(0, str(ROOT / "oracle"))
@@ -366,7 +366,7 @@ def run_reference(args, world):
         "data": "synthetic (seeded R-MAT, no dataset)",
         "config": {"workload": f"R-MAT scale {args.scale}, edge factor {EDGE_FACTOR}, seed {SEED}; six patterns with "
                                "IEP, reference plans; whole-job throughput of the reference CPU path extrapolated "
-                               "from strided start-vertex slices"},
+                               "from strided first-level edge slices"},
         "cpu_baseline": {"value": value, "unit": "embeddings/s", "cores": threads, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": "embeddings/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
