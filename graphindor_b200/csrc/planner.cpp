@@ -303,13 +303,41 @@ Schedule_IEP::Schedule_IEP(const Pattern &pattern, bool &is_pattern_valid, int p
         double min_val = 1e18;
         bool have_best = false;
         const int *src = pattern.get_adj_mat_ptr();
-        for (const auto &vec : candidates) {
+        // The restriction sets and model costs of each order depend only on
+        // the order's adjacency and IEP depth, so they are computed in
+        // parallel on per-thread copies; the orders are then replayed here in
+        // sequence (setup_optimization_info appends to vectors the reference
+        // never clears) and the minimum is taken in the reference's order.
+        struct Eval {
+            std::vector<Pairs> sets;
+            std::vector<double> costs;
+        };
+        std::vector<Eval> evals(candidates.size());
+#pragma omp parallel
+        {
+            Schedule_IEP w;
+            w.alloc(n);
+#pragma omp for schedule(dynamic, 1)
+            for (size_t c = 0; c < candidates.size(); ++c) {
+                w.copy_adj_mat_from(candidates[c], src);
+                w.setup_optimization_info(use_in_exclusion_optimize);
+                Eval &ev = evals[c];
+                w.restricts_generate(ev.sets);
+                if (ev.sets.empty()) {
+                    ev.costs.push_back(w.new_estimate_schedule_restrict(Pairs(), v_cnt, e_cnt, tri_cnt));
+                } else {
+                    for (const auto &pairs : ev.sets)
+                        ev.costs.push_back(w.new_estimate_schedule_restrict(pairs, v_cnt, e_cnt, tri_cnt));
+                }
+            }
+        }
+        for (size_t c = 0; c < candidates.size(); ++c) {
+            const auto &vec = candidates[c];
             copy_adj_mat_from(vec, src);
             setup_optimization_info(use_in_exclusion_optimize);
-            std::vector<Pairs> restricts_vector;
-            restricts_generate(restricts_vector);
-            if (restricts_vector.empty()) {
-                double val = new_estimate_schedule_restrict(Pairs(), v_cnt, e_cnt, tri_cnt);
+            const Eval &ev = evals[c];
+            if (ev.sets.empty()) {
+                const double val = ev.costs[0];
                 if (!have_best || val < min_val) {
                     have_best = true;
                     min_val = val;
@@ -317,13 +345,13 @@ Schedule_IEP::Schedule_IEP(const Pattern &pattern, bool &is_pattern_valid, int p
                     best_pairs.clear();
                 }
             }
-            for (const auto &pairs : restricts_vector) {
-                double val = new_estimate_schedule_restrict(pairs, v_cnt, e_cnt, tri_cnt);
+            for (size_t k = 0; k < ev.sets.size(); ++k) {
+                const double val = ev.costs[k];
                 if (!have_best || val < min_val) {
                     have_best = true;
                     min_val = val;
                     best_order = vec;
-                    best_pairs = pairs;
+                    best_pairs = ev.sets[k];
                 }
             }
         }
@@ -967,22 +995,32 @@ std::vector<Schedule_IEP::Candidate> Schedule_IEP::enumerate_candidates(const Pa
     candidates.erase(std::remove_if(candidates.begin(), candidates.end(),
                                     [&](const std::vector<int> &v) { return s.get_vec_optimize_num(v) != max_val; }),
                      candidates.end());
-    for (const auto &vec : candidates) {
-        s.copy_adj_mat_from(vec, pattern.get_adj_mat_ptr());
-        s.setup_optimization_info(use_iep);
-        std::vector<Pairs> rv;
-        s.restricts_generate(rv);
-        if (rv.empty()) rv.push_back(Pairs());
-        for (const auto &pairs : rv)
-        {
-            std::vector<std::pair<int, int>> applied;
-            for (const auto &p : filter_implied(pairs))
-                if (p.second < n - s.in_exclusion_optimize_num) applied.push_back(p);
-            const int div = restriction_multiplicity(s.adj_mat.data(), n, applied);
-            out.push_back({vec, pairs, s.new_estimate_schedule_restrict(pairs, v_cnt, e_cnt, tri_cnt), div,
-                           s.in_exclusion_optimize_num});
+    // Orders are independent: evaluated in parallel on per-thread copies,
+    // concatenated in order.
+    std::vector<std::vector<Candidate>> per(candidates.size());
+#pragma omp parallel
+    {
+        Schedule_IEP w;
+        w.alloc(n);
+#pragma omp for schedule(dynamic, 1)
+        for (size_t c = 0; c < candidates.size(); ++c) {
+            const auto &vec = candidates[c];
+            w.copy_adj_mat_from(vec, pattern.get_adj_mat_ptr());
+            w.setup_optimization_info(use_iep);
+            std::vector<Pairs> rv;
+            w.restricts_generate(rv);
+            if (rv.empty()) rv.push_back(Pairs());
+            for (const auto &pairs : rv) {
+                std::vector<std::pair<int, int>> applied;
+                for (const auto &p : filter_implied(pairs))
+                    if (p.second < n - w.in_exclusion_optimize_num) applied.push_back(p);
+                const int div = restriction_multiplicity(w.adj_mat.data(), n, applied);
+                per[c].push_back({vec, pairs, w.new_estimate_schedule_restrict(pairs, v_cnt, e_cnt, tri_cnt), div,
+                                  w.in_exclusion_optimize_num});
+            }
         }
     }
+    for (auto &v : per) out.insert(out.end(), v.begin(), v.end());
     return out;
 }
 
