@@ -367,7 +367,7 @@ int gi_plan_candidates(int n, const char *adj, int32_t v_cnt, int64_t e_cnt, int
 // emitted when it is connected and no relabelling of it was emitted before.
 }  // extern "C"
 
-std::vector<std::vector<int>> gi::motif_list(int k) {
+std::vector<std::vector<int>> gi::motif_list(int k, int max_edges) {
     std::vector<std::vector<int>> out;
     std::set<std::set<int>> seen;
     std::vector<std::pair<int, int>> edges;
@@ -400,11 +400,16 @@ std::vector<std::vector<int>> gi::motif_list(int k) {
             return;
         }
         const int i = edges[e].first, j = edges[e].second;
-        edge_set.insert(i * k + j);
-        adj[i * k + j] = adj[j * k + i] = 1;
-        rec(e + 1);
-        adj[i * k + j] = adj[j * k + i] = 0;
-        edge_set.erase(i * k + j);
+        // Patterns over max_edges edges are never emitted; they are not
+        // isomorphic to any kept pattern, so dropping them leaves the kept
+        // patterns, their labellings and their order unchanged.
+        if (static_cast<int>(edge_set.size()) < max_edges) {
+            edge_set.insert(i * k + j);
+            adj[i * k + j] = adj[j * k + i] = 1;
+            rec(e + 1);
+            adj[i * k + j] = adj[j * k + i] = 0;
+            edge_set.erase(i * k + j);
+        }
         rec(e + 1);
     };
     rec(0);

@@ -269,7 +269,7 @@ int plan_patterns(int max_edge, int32_t v_cnt, int64_t e_cnt, int64_t tri_cnt, i
     pats.emplace_back();  // the single vertex
     std::vector<std::pair<int, std::vector<int>>> found;  // (n, adj)
     for (int k = 2; k <= max_edge + 1; ++k)
-        for (auto &adj : motif_list(k))
+        for (auto &adj : motif_list(k, max_edge))
             if (edge_count(adj, k) <= max_edge) found.emplace_back(k, adj);
     std::stable_sort(found.begin(), found.end(), [](const auto &a, const auto &b) {
         return edge_count(a.second, a.first) < edge_count(b.second, b.first);

@@ -16,8 +16,10 @@ namespace gi {
 int fail(int status, const std::string &msg);
 
 // Connected k-vertex patterns (row-major k*k 0/1 matrices) in the order of
-// the reference MotifGenerator; k >= 2.
-std::vector<std::vector<int>> motif_list(int k);
+// the reference MotifGenerator; k >= 2.  With max_edges, only those with at
+// most that many edges (the same patterns, in the same order, as filtering
+// the full list).
+std::vector<std::vector<int>> motif_list(int k, int max_edges = 1 << 30);
 
 // Per-prefix build mode used by the counting kernels.
 enum PrefixMode : int32_t {

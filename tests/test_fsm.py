@@ -88,3 +88,29 @@ def test_fsm_plan_counts_patterns():
     assert [len(gi.fsm_plan(e, 1000, 8000)) for e in (1, 2, 3, 4)] == [1, 2, 5, 10]
     with pytest.raises(gi.GIError):
         gi.fsm_plan(7, 1000, 8000)
+
+
+def _canon(n, adj):
+    import itertools
+    best = None
+    for p in itertools.permutations(range(n)):
+        key = tuple(adj[p[i] * n + p[j]] for i in range(n) for j in range(i + 1, n))
+        if best is None or key > best:
+            best = key
+    return best
+
+
+def test_fsm_pattern_list_for_six_edges_matches_the_filtered_motif_lists():
+    """FSM enumerates motifs with an edge cap; the kept patterns, in order,
+    must be those of the full MotifGenerator lists filtered by edge count."""
+    plans = gi.fsm_plan(6, 50000, 1000000)
+    want = [(2, "0110")]
+    for k in range(3, 8):
+        for a in (gi.motif_patterns(k) if k < 7 else []):
+            if sum(a[i * k + j] == "1" for i in range(k) for j in range(i + 1, k)) <= 6:
+                want.append((k, a))
+    got7 = [p for p in plans if p["n"] == 7]
+    assert len(got7) == 11  # the trees on 7 vertices
+    got = [p for p in plans if p["n"] < 7]
+    want_e = sorted(want, key=lambda t: sum(t[1][i * t[0] + j] == "1" for i in range(t[0]) for j in range(i + 1, t[0])))
+    assert [(p["n"], _canon(p["n"], p["adj"])) for p in got] == [(n, _canon(n, a)) for n, a in want_e]
