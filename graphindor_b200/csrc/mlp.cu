@@ -214,6 +214,31 @@ int gi_mlp_grad(const float *X, const float *y, int rows, int in, int hidden, co
     return GI_OK;
 }
 
+int gi_mlp_predict(const float *X, int rows, int in, int hidden, const float *params, float *y_out) {
+    if (!X || !params || !y_out || rows < 1 || in < 1 || hidden < 1 || hidden > 1024)
+        return fail(GI_EINVAL, "bad MLP arguments");
+    const MlpShape s = shape_of(in, hidden);
+    Dev d;
+    float *dX, *dP, *H1, *H2, *Y;
+    int32_t *dI;
+    cudaError_t e;
+    std::vector<int32_t> idx(rows);
+    std::iota(idx.begin(), idx.end(), 0);
+    if ((e = d.alloc(&dX, static_cast<size_t>(rows) * in)) != cudaSuccess || (e = d.alloc(&dP, s.total)) != cudaSuccess ||
+        (e = d.alloc(&dI, rows)) != cudaSuccess || (e = d.alloc(&H1, static_cast<size_t>(rows) * hidden)) != cudaSuccess ||
+        (e = d.alloc(&H2, static_cast<size_t>(rows) * hidden)) != cudaSuccess || (e = d.alloc(&Y, rows)) != cudaSuccess)
+        return cuda_fail(e, "MLP allocation");
+    if ((e = cudaMemcpy(dX, X, sizeof(float) * rows * in, cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (e = cudaMemcpy(dP, params, sizeof(float) * s.total, cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (e = cudaMemcpy(dI, idx.data(), sizeof(int32_t) * rows, cudaMemcpyHostToDevice)) != cudaSuccess)
+        return cuda_fail(e, "MLP upload");
+    mlp_fwd_kernel<<<rows, hidden, 2 * sizeof(float) * hidden>>>(s, dP, dX, dI, rows, H1, H2, Y);
+    if ((e = cudaGetLastError()) != cudaSuccess ||
+        (e = cudaMemcpy(y_out, Y, sizeof(float) * rows, cudaMemcpyDeviceToHost)) != cudaSuccess)
+        return cuda_fail(e, "MLP forward");
+    return GI_OK;
+}
+
 int gi_mlp_train(const float *X, const float *y, int rows, int in, int hidden, int epochs, int batch, float lr,
                  float wd, uint64_t seed, float *params_inout, float *loss_out) {
     if (!X || !y || !params_inout || rows < 1 || in < 1 || hidden < 1 || hidden > 1024 || epochs < 0 || batch < 1)

@@ -309,6 +309,9 @@ int gi_plan_create_learned(int n, const char *adj, int32_t v_cnt, int64_t e_cnt,
  * rows. */
 int gi_mlp_grad(const float *X, const float *y, int rows, int in, int hidden, const float *params, float *grad_out,
                 float *loss_out);
+/* The model's output (log10 predicted ms) for each of `rows` normalised
+ * feature rows, on the GPU. */
+int gi_mlp_predict(const float *X, int rows, int in, int hidden, const float *params, float *y_out);
 int gi_mlp_train(const float *X, const float *y, int rows, int in, int hidden, int epochs, int batch, float lr,
                  float wd, uint64_t seed, float *params_inout, float *loss_out);
 

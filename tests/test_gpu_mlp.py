@@ -50,3 +50,18 @@ def test_gpu_training_fits_like_the_host_trainer():
     host_loss = float(np.mean((hp - y) ** 2))
     assert final < 0.25 * loss0
     assert final < 2.0 * host_loss + 1e-3
+
+
+def test_gpu_inference_matches_the_host_forward():
+    """The shipped model's predictions on the committed feature rows, GPU
+    against host."""
+    here = Path(gi.__file__).resolve().parent / "schedule_cost"
+    X, _, _, _, _ = train.load_rows(str(here / "runs_b200.json"))
+    mlp, mu, sd = train.load(str(here / "weights.bin"))
+    Xn = np.ascontiguousarray((X - mu) / sd, dtype=np.float32)
+    p = mlp.pack()
+    out = np.zeros(len(Xn), dtype=np.float32)
+    N.check(gi.lib().gi_mlp_predict(Xn.ctypes.data, len(Xn), DIM, train.HIDDEN, p.ctypes.data, out.ctypes.data),
+            "gi_mlp_predict")
+    want, _ = mlp.forward(Xn)
+    assert np.allclose(out, want, rtol=1e-4, atol=1e-4)
