@@ -673,3 +673,139 @@ int oracle_fsm_support(int32_t v_cnt, int32_t l_cnt, const uint32_t *bucket, con
     }
     return 0;
 }
+
+/* ------------------------------------------------- clique-tree pivoting */
+
+typedef struct {
+    const int64_t *vertex;
+    const int32_t *edge;
+    int kmax;
+    uint64_t binom[64][64];
+    uint64_t acc[GI_MAX_PATTERN + 1];
+    int32_t **lvl;  /* candidate buffers per recursion level */
+    int32_t *tmp;
+} pivot_t;
+
+static int sorted_has(const int32_t *a, int64_t n, int32_t x) {
+    int64_t lo = 0, hi = n;
+    while (lo < hi) {
+        const int64_t mid = (lo + hi) / 2;
+        if (a[mid] < x) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo < n && a[lo] == x;
+}
+
+/* |S ∩ N(x)| and, when out != NULL, the intersection itself (S sorted). */
+static int64_t inter(const pivot_t *t, const int32_t *S, int64_t n, int32_t x, int32_t *out) {
+    const int32_t *nb = t->edge + t->vertex[x];
+    const int64_t dn = t->vertex[x + 1] - t->vertex[x];
+    int64_t c = 0, i = 0, j = 0;
+    while (i < n && j < dn) {
+        if (S[i] < nb[j]) ++i;
+        else if (S[i] > nb[j]) ++j;
+        else {
+            if (out) out[c] = S[i];
+            ++c;
+            ++i;
+            ++j;
+        }
+    }
+    return c;
+}
+
+static void pivot_rec(pivot_t *t, const int32_t *S, int64_t n, int h, int q, int depth) {
+    if (h > t->kmax) return;
+    if (n == 0) {
+        for (int k = h; k <= t->kmax && k - h <= q; ++k) t->acc[k] += t->binom[q][k - h];
+        return;
+    }
+    int64_t best = -1;
+    int32_t u = S[0];
+    for (int64_t i = 0; i < n; ++i) {
+        const int64_t c = inter(t, S, n, S[i], NULL);
+        if (c > best) {
+            best = c;
+            u = S[i];
+        }
+    }
+    int32_t *next = t->lvl[depth + 1];
+    int64_t m = inter(t, S, n, u, next);
+    pivot_rec(t, next, m, h, q + 1, depth + 1);
+    /* Non-neighbours of u other than u, in order; each excludes the earlier ones. */
+    int32_t *rest = t->lvl[depth] + n;  /* the level's spare half */
+    int64_t nr = 0;
+    for (int64_t i = 0; i < n; ++i) rest[nr++] = S[i];
+    for (int64_t i = 0; i < n; ++i) {
+        const int32_t w = S[i];
+        if (w == u || sorted_has(t->edge + t->vertex[u], t->vertex[u + 1] - t->vertex[u], w)) continue;
+        /* rest holds S minus the earlier non-neighbours, still sorted */
+        int64_t r = 0;
+        for (int64_t j = 0; j < nr; ++j)
+            if (rest[j] != w) rest[r++] = rest[j];
+        m = inter(t, rest, r, w, next);
+        pivot_rec(t, next, m, h + 1, q, depth + 1);
+        nr = r;
+    }
+}
+
+int oracle_clique_counts_pivot(int kmax, const int64_t *vertex, const int32_t *edge, int32_t v_cnt, int threads,
+                               uint64_t *out) {
+    if (kmax < 1 || kmax > GI_MAX_PATTERN || v_cnt < 1) return -1;
+    /* Candidate sets are subsets of a vertex's later neighbours, and every
+     * level of the recursion adds a vertex adjacent to all the earlier ones,
+     * so the largest later-neighbour count bounds both set sizes and depth. */
+    int64_t dmax = 0;
+    for (int32_t v = 0; v < v_cnt; ++v) {
+        const int64_t dv = vertex[v + 1] - vertex[v];
+        int64_t later = 0;
+        for (int64_t e = vertex[v]; e < vertex[v + 1]; ++e) {
+            const int64_t dw = vertex[edge[e] + 1] - vertex[edge[e]];
+            later += dw > dv || (dw == dv && edge[e] > v);
+        }
+        if (later > dmax) dmax = later;
+    }
+    for (int k = 0; k <= kmax; ++k) out[k] = 0;
+    if (threads <= 0) threads = omp_get_max_threads();
+    int fail = 0;
+#pragma omp parallel num_threads(threads)
+    {
+        pivot_t t;
+        memset(&t, 0, sizeof(t));
+        t.vertex = vertex;
+        t.edge = edge;
+        t.kmax = kmax;
+        for (int a = 0; a < 64; ++a) {
+            t.binom[a][0] = 1;
+            for (int b = 1; b <= a; ++b) t.binom[a][b] = t.binom[a - 1][b - 1] + (b < a ? t.binom[a - 1][b] : 0);
+        }
+        /* Depth is at most dmax + 1 levels; each level holds a candidate set
+         * and a spare copy. */
+        const int64_t levels = dmax + 2;
+        t.lvl = (int32_t **)malloc(sizeof(int32_t *) * levels);
+        int32_t *pool = (int32_t *)malloc(sizeof(int32_t) * (size_t)levels * (size_t)(2 * dmax + 2));
+        if (!t.lvl || !pool) {
+#pragma omp atomic write
+            fail = 1;
+        } else {
+            for (int64_t l = 0; l < levels; ++l) t.lvl[l] = pool + l * (2 * dmax + 2);
+#pragma omp for schedule(dynamic, 64)
+            for (int32_t v = 0; v < v_cnt; ++v) {
+                const int64_t dv = vertex[v + 1] - vertex[v];
+                /* later neighbours in (degree, id) order */
+                int64_t n = 0;
+                for (int64_t e = vertex[v]; e < vertex[v + 1]; ++e) {
+                    const int32_t w = edge[e];
+                    const int64_t dw = vertex[w + 1] - vertex[w];
+                    if (dw > dv || (dw == dv && w > v)) t.lvl[0][n++] = w;
+                }
+                pivot_rec(&t, t.lvl[0], n, 1, 0, 0);
+            }
+        }
+#pragma omp critical
+        for (int k = 0; k <= kmax; ++k) out[k] += t.acc[k];
+        free(t.lvl);
+        free(pool);
+    }
+    return fail ? -1 : 0;
+}

@@ -66,6 +66,19 @@ uint64_t oracle_brute_count(int n, const char *adj, int induced, const int64_t *
  * tuples.  For small graphs only. */
 uint64_t oracle_clique_count(int k, const int64_t *vertex, const int32_t *edge, int32_t v_cnt);
 
+/* Number of k-cliques for every k in [1, kmax] at once (out[k], modulo 2^64;
+ * out needs kmax + 1 entries) by clique-tree pivoting (Jain and Seshadhri,
+ * "The Power of Pivoting for Exact Clique Counting", WSDM 2020): vertices in
+ * (degree, id) order; for each v the candidates are its later neighbours; a
+ * node with candidates S picks the pivot u of S with the most neighbours in S
+ * and has one child S ∩ N(u) in which u is optional, and one child per other
+ * w ∈ S \ N(u), S ∩ N(w) minus the earlier such w, in which w is required.
+ * A leaf with h required and q optional vertices holds C(q, k - h)
+ * k-cliques.  An independent check of the engine's k-clique counts for large
+ * k, where enumeration is too slow.  Returns 0, or -1 on bad input. */
+int oracle_clique_counts_pivot(int kmax, const int64_t *vertex, const int32_t *edge, int32_t v_cnt, int threads,
+                               uint64_t *out);
+
 /* Exact triangle count (each triangle once) by merging sorted lists,
  * reference src/graph.cpp:1006-1043 (motif_counting_3). */
 uint64_t oracle_triangles(const int64_t *vertex, const int32_t *edge, int32_t v_cnt, int threads);

@@ -117,6 +117,22 @@ def cliques(k, vertex, edge):
     return lib().oracle_clique_count(k, vertex.ctypes.data, edge.ctypes.data, len(vertex) - 1)
 
 
+def clique_counts_pivot(kmax, vertex, edge, threads=0):
+    """[count of k-cliques for k = 0 .. kmax] (index 0 unused) by clique-tree
+    pivoting, modulo 2^64."""
+    L_ = lib()
+    if not hasattr(L_.oracle_clique_counts_pivot, "_typed"):
+        L_.oracle_clique_counts_pivot.restype = C.c_int
+        L_.oracle_clique_counts_pivot.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_int32, C.c_int, C.c_void_p]
+        L_.oracle_clique_counts_pivot._typed = True
+    vertex, edge = _arrays(vertex, edge)
+    out = np.zeros(kmax + 1, dtype=np.uint64)
+    if L_.oracle_clique_counts_pivot(kmax, vertex.ctypes.data, edge.ctypes.data, len(vertex) - 1, threads,
+                                     out.ctypes.data) != 0:
+        raise ValueError("oracle_clique_counts_pivot failed")
+    return [int(x) for x in out]
+
+
 def triangles(vertex, edge, threads=0):
     vertex, edge = _arrays(vertex, edge)
     return lib().oracle_triangles(vertex.ctypes.data, edge.ctypes.data, len(vertex) - 1, threads)

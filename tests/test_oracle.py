@@ -130,3 +130,15 @@ def test_oracle_wiki_vote_vectors(oracle):
                          (4, "0110100110010110", 57654491), (5, "0111110111110111110111110", 4514137)]:
         got, _ = _oracle_count(oracle, g, n, adj)
         assert got == want
+
+
+def test_pivoting_clique_counts_match_enumeration(oracle):
+    """The clique-tree pivoting oracle (exact counts for large k) against the
+    enumerating one and against C(n, k) on a complete graph."""
+    from math import comb
+    from graphindor_b200 import gen
+    for g in (gen.erdos_renyi(200, 3000, 1), gen.rmat(9, 8.0, 11), gen.chung_lu(2000, 12000, 2.2, 200.0, 14)):
+        piv = oracle.clique_counts_pivot(7, g.vertex, g.edge)
+        assert piv[3:7] == [oracle.cliques(k, g.vertex, g.edge) for k in range(3, 7)]
+    k40 = gen.from_edges(40, [(i, j) for i in range(40) for j in range(i + 1, 40)])
+    assert oracle.clique_counts_pivot(7, k40.vertex, k40.edge)[1:] == [comb(40, k) for k in range(1, 8)]
