@@ -676,85 +676,92 @@ int oracle_fsm_support(int32_t v_cnt, int32_t l_cnt, const uint32_t *bucket, con
 
 /* ------------------------------------------------- clique-tree pivoting */
 
+/* One root's search: the candidates are the root's later neighbours, numbered
+ * 0..n-1 in id order; adj[i] is row i of their induced adjacency as a bit
+ * row of W words.  Candidate sets are bit rows too, one per recursion depth
+ * (cand), with a spare row per depth for the non-neighbour children (rest). */
 typedef struct {
-    const int64_t *vertex;
-    const int32_t *edge;
     int kmax;
-    uint64_t binom[64][64];
+    int64_t W;
+    uint64_t *adj;
+    uint64_t *cand;
+    uint64_t *rest;
+    const uint64_t *binom; /* binom[q * (kmax + 1) + j] = C(q, j) modulo 2^64 */
     uint64_t acc[GI_MAX_PATTERN + 1];
-    int32_t **lvl;  /* candidate buffers per recursion level */
-    int32_t *tmp;
 } pivot_t;
 
-static int sorted_has(const int32_t *a, int64_t n, int32_t x) {
-    int64_t lo = 0, hi = n;
-    while (lo < hi) {
-        const int64_t mid = (lo + hi) / 2;
-        if (a[mid] < x) lo = mid + 1;
-        else hi = mid;
-    }
-    return lo < n && a[lo] == x;
-}
-
-/* |S ∩ N(x)| and, when out != NULL, the intersection itself (S sorted). */
-static int64_t inter(const pivot_t *t, const int32_t *S, int64_t n, int32_t x, int32_t *out) {
-    const int32_t *nb = t->edge + t->vertex[x];
-    const int64_t dn = t->vertex[x + 1] - t->vertex[x];
-    int64_t c = 0, i = 0, j = 0;
-    while (i < n && j < dn) {
-        if (S[i] < nb[j]) ++i;
-        else if (S[i] > nb[j]) ++j;
-        else {
-            if (out) out[c] = S[i];
-            ++c;
-            ++i;
-            ++j;
-        }
-    }
+static int64_t row_popcount_and(const uint64_t *a, const uint64_t *b, int64_t W) {
+    int64_t c = 0;
+    for (int64_t i = 0; i < W; ++i) c += __builtin_popcountll(a[i] & b[i]);
     return c;
 }
 
-static void pivot_rec(pivot_t *t, const int32_t *S, int64_t n, int h, int q, int depth) {
-    if (h > t->kmax) return;
-    if (n == 0) {
-        for (int k = h; k <= t->kmax && k - h <= q; ++k) t->acc[k] += t->binom[q][k - h];
+/* Node with candidate row cand[depth], h required and q optional vertices. */
+static void pivot_rec(pivot_t *t, int64_t depth, int h, int64_t q) {
+    const int64_t W = t->W;
+    const uint64_t *S = t->cand + depth * W;
+    const int K1 = t->kmax + 1;
+    if (h >= t->kmax - 2) {
+        /* The subtree of this node counts every clique R ∪ P' ∪ C once, R the
+         * h required vertices, P' a subset of the q optional ones and C a
+         * clique of G[S].  With at most two vertices left to add up to kmax,
+         * the k-clique count is sum_j C(q, j) cl(k - h - j), where cl(0) = 1,
+         * cl(1) = |S| and cl(2) = the edges of G[S]; no descent needed. */
+        uint64_t cl[3] = {1, 0, 0};
+        for (int64_t w = 0; w < W; ++w) cl[1] += (uint64_t)__builtin_popcountll(S[w]);
+        if (h == t->kmax - 2) {
+            uint64_t twice = 0;
+            for (int64_t w = 0; w < W; ++w)
+                for (uint64_t b = S[w]; b; b &= b - 1)
+                    twice += (uint64_t)row_popcount_and(S, t->adj + (w * 64 + __builtin_ctzll(b)) * W, W);
+            cl[2] = twice / 2;
+        }
+        for (int k = h; k <= t->kmax; ++k)
+            for (int j = 0; j <= k - h && j <= q; ++j) t->acc[k] += t->binom[q * K1 + j] * cl[k - h - j];
         return;
     }
-    int64_t best = -1;
-    int32_t u = S[0];
-    for (int64_t i = 0; i < n; ++i) {
-        const int64_t c = inter(t, S, n, S[i], NULL);
-        if (c > best) {
-            best = c;
-            u = S[i];
+    int64_t u = -1, best = -1;
+    for (int64_t w = 0; w < W; ++w)
+        for (uint64_t b = S[w]; b; b &= b - 1) {
+            const int64_t x = w * 64 + __builtin_ctzll(b);
+            const int64_t c = row_popcount_and(S, t->adj + x * W, W);
+            if (c > best) {
+                best = c;
+                u = x;
+            }
         }
+    if (u < 0) { /* leaf */
+        for (int k = h; k <= t->kmax && k - h <= q; ++k) t->acc[k] += t->binom[q * K1 + (k - h)];
+        return;
     }
-    int32_t *next = t->lvl[depth + 1];
-    int64_t m = inter(t, S, n, u, next);
-    pivot_rec(t, next, m, h, q + 1, depth + 1);
-    /* Non-neighbours of u other than u, in order; each excludes the earlier ones. */
-    int32_t *rest = t->lvl[depth] + n;  /* the level's spare half */
-    int64_t nr = 0;
-    for (int64_t i = 0; i < n; ++i) rest[nr++] = S[i];
-    for (int64_t i = 0; i < n; ++i) {
-        const int32_t w = S[i];
-        if (w == u || sorted_has(t->edge + t->vertex[u], t->vertex[u + 1] - t->vertex[u], w)) continue;
-        /* rest holds S minus the earlier non-neighbours, still sorted */
-        int64_t r = 0;
-        for (int64_t j = 0; j < nr; ++j)
-            if (rest[j] != w) rest[r++] = rest[j];
-        m = inter(t, rest, r, w, next);
-        pivot_rec(t, next, m, h + 1, q, depth + 1);
-        nr = r;
+    uint64_t *next = t->cand + (depth + 1) * W;
+    const uint64_t *au = t->adj + u * W;
+    for (int64_t w = 0; w < W; ++w) next[w] = S[w] & au[w];
+    pivot_rec(t, depth + 1, h, q + 1);
+    /* Each non-neighbour w of u other than u is required in its child, whose
+     * candidates are S ∩ N(w) minus the earlier such w. */
+    uint64_t *cur = t->rest + depth * W;
+    for (int64_t w = 0; w < W; ++w) cur[w] = S[w];
+    for (int64_t w = 0; w < W; ++w) {
+        uint64_t b = S[w] & ~au[w];
+        if (w == u / 64) b &= ~(1ull << (u % 64));
+        for (; b; b &= b - 1) {
+            const int64_t x = w * 64 + __builtin_ctzll(b);
+            const uint64_t *ax = t->adj + x * W;
+            for (int64_t i = 0; i < W; ++i) next[i] = cur[i] & ax[i];
+            pivot_rec(t, depth + 1, h + 1, q);
+            cur[w] &= ~(1ull << (x % 64));
+        }
     }
 }
 
 int oracle_clique_counts_pivot(int kmax, const int64_t *vertex, const int32_t *edge, int32_t v_cnt, int threads,
                                uint64_t *out) {
     if (kmax < 1 || kmax > GI_MAX_PATTERN || v_cnt < 1) return -1;
-    /* Candidate sets are subsets of a vertex's later neighbours, and every
-     * level of the recursion adds a vertex adjacent to all the earlier ones,
-     * so the largest later-neighbour count bounds both set sizes and depth. */
+    /* Later neighbours in (degree, id) order, each list in id order. */
+    int64_t *off = (int64_t *)malloc(sizeof(int64_t) * ((size_t)v_cnt + 1));
+    if (!off) return -1;
+    off[0] = 0;
     int64_t dmax = 0;
     for (int32_t v = 0; v < v_cnt; ++v) {
         const int64_t dv = vertex[v + 1] - vertex[v];
@@ -763,49 +770,84 @@ int oracle_clique_counts_pivot(int kmax, const int64_t *vertex, const int32_t *e
             const int64_t dw = vertex[edge[e] + 1] - vertex[edge[e]];
             later += dw > dv || (dw == dv && edge[e] > v);
         }
+        off[v + 1] = off[v] + later;
         if (later > dmax) dmax = later;
     }
+    int32_t *out_nb = (int32_t *)malloc(sizeof(int32_t) * ((size_t)off[v_cnt] + 1));
+    /* Every vertex chosen along a path of the recursion is adjacent to all the
+     * later candidates, so the depth (and q) is at most dmax + 1. */
+    const int64_t qmax = dmax + 2;
+    uint64_t *binom = (uint64_t *)malloc(sizeof(uint64_t) * (size_t)(qmax + 1) * (size_t)(kmax + 1));
+    if (!out_nb || !binom) {
+        free(off);
+        free(out_nb);
+        free(binom);
+        return -1;
+    }
+    for (int32_t v = 0; v < v_cnt; ++v) {
+        const int64_t dv = vertex[v + 1] - vertex[v];
+        int64_t o = off[v];
+        for (int64_t e = vertex[v]; e < vertex[v + 1]; ++e) {
+            const int32_t w = edge[e];
+            const int64_t dw = vertex[w + 1] - vertex[w];
+            if (dw > dv || (dw == dv && w > v)) out_nb[o++] = w;
+        }
+    }
+    for (int64_t a = 0; a <= qmax; ++a)
+        for (int b = 0; b <= kmax; ++b)
+            binom[a * (kmax + 1) + b] =
+                b == 0 ? 1 : (a == 0 ? 0 : binom[(a - 1) * (kmax + 1) + b - 1] + binom[(a - 1) * (kmax + 1) + b]);
     for (int k = 0; k <= kmax; ++k) out[k] = 0;
     if (threads <= 0) threads = omp_get_max_threads();
     int fail = 0;
+    const int64_t Wmax = (dmax + 63) / 64 > 0 ? (dmax + 63) / 64 : 1;
 #pragma omp parallel num_threads(threads)
     {
         pivot_t t;
         memset(&t, 0, sizeof(t));
-        t.vertex = vertex;
-        t.edge = edge;
         t.kmax = kmax;
-        for (int a = 0; a < 64; ++a) {
-            t.binom[a][0] = 1;
-            for (int b = 1; b <= a; ++b) t.binom[a][b] = t.binom[a - 1][b - 1] + (b < a ? t.binom[a - 1][b] : 0);
-        }
-        /* Depth is at most dmax + 1 levels; each level holds a candidate set
-         * and a spare copy. */
-        const int64_t levels = dmax + 2;
-        t.lvl = (int32_t **)malloc(sizeof(int32_t *) * levels);
-        int32_t *pool = (int32_t *)malloc(sizeof(int32_t) * (size_t)levels * (size_t)(2 * dmax + 2));
-        if (!t.lvl || !pool) {
+        t.binom = binom;
+        const int64_t levels = dmax + 3;
+        t.adj = (uint64_t *)malloc(sizeof(uint64_t) * (size_t)(dmax > 0 ? dmax : 1) * (size_t)Wmax);
+        t.cand = (uint64_t *)malloc(sizeof(uint64_t) * (size_t)levels * (size_t)Wmax);
+        t.rest = (uint64_t *)malloc(sizeof(uint64_t) * (size_t)levels * (size_t)Wmax);
+        int32_t *pos = (int32_t *)calloc((size_t)v_cnt, sizeof(int32_t)); /* local index + 1, or 0 */
+        if (!t.adj || !t.cand || !t.rest || !pos) {
 #pragma omp atomic write
             fail = 1;
         } else {
-            for (int64_t l = 0; l < levels; ++l) t.lvl[l] = pool + l * (2 * dmax + 2);
 #pragma omp for schedule(dynamic, 64)
             for (int32_t v = 0; v < v_cnt; ++v) {
-                const int64_t dv = vertex[v + 1] - vertex[v];
-                /* later neighbours in (degree, id) order */
-                int64_t n = 0;
-                for (int64_t e = vertex[v]; e < vertex[v + 1]; ++e) {
-                    const int32_t w = edge[e];
-                    const int64_t dw = vertex[w + 1] - vertex[w];
-                    if (dw > dv || (dw == dv && w > v)) t.lvl[0][n++] = w;
-                }
-                pivot_rec(&t, t.lvl[0], n, 1, 0, 0);
+                const int32_t *L = out_nb + off[v];
+                const int64_t n = off[v + 1] - off[v];
+                const int64_t W = t.W = n > 64 ? (n + 63) / 64 : 1; /* row width of this root */
+                for (int64_t i = 0; i < n; ++i) pos[L[i]] = (int32_t)(i + 1);
+                memset(t.adj, 0, sizeof(uint64_t) * (size_t)n * (size_t)W);
+                /* Both ends of an edge inside L: the later one is in the
+                 * earlier one's out-list. */
+                for (int64_t i = 0; i < n; ++i)
+                    for (int64_t e = off[L[i]]; e < off[L[i] + 1]; ++e) {
+                        const int32_t p = pos[out_nb[e]];
+                        if (!p) continue;
+                        const int64_t j = p - 1;
+                        t.adj[i * W + j / 64] |= 1ull << (j % 64);
+                        t.adj[j * W + i / 64] |= 1ull << (i % 64);
+                    }
+                memset(t.cand, 0, sizeof(uint64_t) * (size_t)W);
+                for (int64_t i = 0; i < n; ++i) t.cand[i / 64] |= 1ull << (i % 64);
+                pivot_rec(&t, 0, 1, 0);
+                for (int64_t i = 0; i < n; ++i) pos[L[i]] = 0;
             }
         }
 #pragma omp critical
         for (int k = 0; k <= kmax; ++k) out[k] += t.acc[k];
-        free(t.lvl);
-        free(pool);
+        free(t.adj);
+        free(t.cand);
+        free(t.rest);
+        free(pos);
     }
+    free(off);
+    free(out_nb);
+    free(binom);
     return fail ? -1 : 0;
 }

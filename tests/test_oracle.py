@@ -140,5 +140,13 @@ def test_pivoting_clique_counts_match_enumeration(oracle):
     for g in (gen.erdos_renyi(200, 3000, 1), gen.rmat(9, 8.0, 11), gen.chung_lu(2000, 12000, 2.2, 200.0, 14)):
         piv = oracle.clique_counts_pivot(7, g.vertex, g.edge)
         assert piv[3:7] == [oracle.cliques(k, g.vertex, g.edge) for k in range(3, 7)]
+        for kmax in (3, 5):  # stopping at h = kmax leaves the lower counts as they are
+            assert oracle.clique_counts_pivot(kmax, g.vertex, g.edge) == piv[:kmax + 1]
     k40 = gen.from_edges(40, [(i, j) for i in range(40) for j in range(i + 1, 40)])
     assert oracle.clique_counts_pivot(7, k40.vertex, k40.edge)[1:] == [comb(40, k) for k in range(1, 8)]
+    # Cliques longer than one 64-bit row word, with a pendant path attached.
+    k70 = gen.from_edges(73, [(i, j) for i in range(70) for j in range(i + 1, 70)] + [(69, 70), (70, 71), (71, 72)])
+    want = [comb(70, k) for k in range(1, 8)]
+    want[0] += 3
+    want[1] += 3
+    assert oracle.clique_counts_pivot(7, k70.vertex, k70.edge)[1:] == want
