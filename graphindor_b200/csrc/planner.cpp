@@ -12,7 +12,10 @@
 #include <cmath>
 #include <cstring>
 #include <map>
+#include <memory>
+#include <mutex>
 #include <numeric>
+#include <tuple>
 
 namespace gi {
 
@@ -72,14 +75,19 @@ bool Pattern::is_dag() const {
 namespace {
 
 // All permutations of 0..n-1 in lexicographic order (the order of the
-// reference's get_full_permutation DFS).
-std::vector<std::vector<int>> all_permutations(int n) {
-    std::vector<std::vector<int>> out;
-    std::vector<int> p(n);
-    std::iota(p.begin(), p.end(), 0);
-    do out.push_back(p);
-    while (std::next_permutation(p.begin(), p.end()));
-    return out;
+// reference's get_full_permutation DFS), built once per n.
+const std::vector<std::vector<int>> &all_permutations(int n) {
+    static const std::vector<std::vector<std::vector<int>>> table = [] {
+        std::vector<std::vector<std::vector<int>>> t(kMaxPatternSize + 1);
+        for (int m = 0; m <= kMaxPatternSize; ++m) {
+            std::vector<int> p(m);
+            std::iota(p.begin(), p.end(), 0);
+            do t[m].push_back(p);
+            while (std::next_permutation(p.begin(), p.end()));
+        }
+        return t;
+    }();
+    return table.at(n);
 }
 
 // Cycle decomposition of a permutation, cycles listed from their smallest
@@ -240,6 +248,49 @@ int restriction_multiplicity(const int *adj, int n, const std::vector<std::pair<
 
 // ---------------------------------------------------------- Schedule_IEP
 
+// Pattern-only state of the model constructor, shared by every plan of the
+// same pattern (any graph).  Bounded: the whole cache is dropped when it
+// holds more than kModelCacheEntries patterns.
+struct Schedule_IEP::ModelKey {
+    int n;
+    uint64_t adj;
+    bool use_iep;
+    bool vertex_induced;
+    bool operator<(const ModelKey &o) const {
+        return std::tie(n, adj, use_iep, vertex_induced) < std::tie(o.n, o.adj, o.use_iep, o.vertex_induced);
+    }
+};
+
+struct Schedule_IEP::ModelState {
+    std::vector<std::vector<int>> candidates;  // orders of maximal IEP depth, in enumeration order
+    std::vector<std::vector<Pairs>> sets;      // restriction sets per order
+    std::vector<int> iep_num;                  // IEP depth per order
+    std::vector<int> rep;                      // first order with the same ordered adjacency (same scores)
+    std::unique_ptr<const Schedule_IEP> replayed;  // state after the replay of every order
+    mutable std::mutex mu;
+    mutable std::map<std::pair<int, int>, long long> redundancy;  // by chosen (order, set); set -1 = none
+};
+
+namespace {
+constexpr size_t kModelCacheEntries = 4096;
+std::mutex g_model_mu;
+std::map<Schedule_IEP::ModelKey, std::shared_ptr<const Schedule_IEP::ModelState>> g_model_cache;
+}  // namespace
+
+std::shared_ptr<const Schedule_IEP::ModelState> Schedule_IEP::model_cache_find(const ModelKey &k) {
+    std::lock_guard<std::mutex> lock(g_model_mu);
+    auto it = g_model_cache.find(k);
+    return it == g_model_cache.end() ? nullptr : it->second;
+}
+
+std::shared_ptr<const Schedule_IEP::ModelState> Schedule_IEP::model_cache_insert(const ModelKey &k,
+                                                                                std::shared_ptr<ModelState> s) {
+    std::lock_guard<std::mutex> lock(g_model_mu);
+    if (g_model_cache.size() >= kModelCacheEntries) g_model_cache.clear();
+    return g_model_cache.emplace(k, std::move(s)).first->second;
+}
+
+
 void Schedule_IEP::alloc(int n) {
     size = n;
     const int maxp = n * (n - 1) / 2 + 1;
@@ -285,73 +336,116 @@ Schedule_IEP::Schedule_IEP(const Pattern &pattern, bool &is_pattern_valid, int p
     }
 
     Pairs best_pairs;
+    std::shared_ptr<const ModelState> st;  // model path: the pattern's cached state
+    std::pair<int, int> best_ck(-1, -1);   // model path: chosen (order, restriction set) index
     if (performance_modeling_type != 0) {
-        auto candidates = all_permutations(n);
-        // reference src/schedule_IEP.cpp:2019-2042: every position after the
-        // first must touch an earlier one.
-        candidates.erase(std::remove_if(candidates.begin(), candidates.end(),
-                                        [&](const std::vector<int> &v) { return get_vec_optimize_num(v) < 0; }),
-                         candidates.end());
-        int max_val = 0;
-        for (const auto &v : candidates) max_val = std::max(max_val, get_vec_optimize_num(v));
-        k_val = max_val;
-        candidates.erase(std::remove_if(candidates.begin(), candidates.end(),
-                                        [&](const std::vector<int> &v) { return get_vec_optimize_num(v) != max_val; }),
-                         candidates.end());
-
-        std::vector<int> best_order(n, 0);
-        double min_val = 1e18;
-        bool have_best = false;
         const int *src = pattern.get_adj_mat_ptr();
-        // The restriction sets and model costs of each order depend only on
-        // the order's adjacency and IEP depth, so they are computed in
-        // parallel on per-thread copies; the orders are then replayed here in
-        // sequence (setup_optimization_info appends to vectors the reference
-        // never clears) and the minimum is taken in the reference's order.
-        struct Eval {
-            std::vector<Pairs> sets;
-            std::vector<double> costs;
-        };
-        std::vector<Eval> evals(candidates.size());
+        // Everything the model loop does apart from scoring depends on the
+        // pattern alone: the candidate orders, their restriction sets and
+        // IEP depths, and the state the sequential replay leaves behind (the
+        // never-cleared IEP vectors and prefix flags).  It is computed once
+        // per pattern and reused for every graph; only the scores are
+        // recomputed from (v_cnt, e_cnt, tri_cnt).
+        const ModelKey key{n, adj_key(src, n), use_in_exclusion_optimize, vertex_induced};
+        st = model_cache_find(key);
+        if (st) {
+            *this = *st->replayed;
+        } else {
+            auto ns = std::make_shared<ModelState>();
+            auto candidates = all_permutations(n);
+            // reference src/schedule_IEP.cpp:2019-2042: every position after
+            // the first must touch an earlier one.
+            candidates.erase(std::remove_if(candidates.begin(), candidates.end(),
+                                            [&](const std::vector<int> &v) { return get_vec_optimize_num(v) < 0; }),
+                             candidates.end());
+            int max_val = 0;
+            for (const auto &v : candidates) max_val = std::max(max_val, get_vec_optimize_num(v));
+            k_val = max_val;
+            candidates.erase(std::remove_if(candidates.begin(), candidates.end(),
+                                            [&](const std::vector<int> &v) {
+                                                return get_vec_optimize_num(v) != max_val;
+                                            }),
+                             candidates.end());
+            ns->sets.resize(candidates.size());
+            ns->iep_num.resize(candidates.size());
+            // Restriction sets per order, on per-thread copies in parallel.
+#pragma omp parallel
+            {
+                Schedule_IEP w;
+                w.alloc(n);
+#pragma omp for schedule(dynamic, 1)
+                for (size_t c = 0; c < candidates.size(); ++c) {
+                    w.copy_adj_mat_from(candidates[c], src);
+                    w.setup_optimization_info(use_in_exclusion_optimize);
+                    w.restricts_generate(ns->sets[c]);
+                    ns->iep_num[c] = w.in_exclusion_optimize_num;
+                }
+            }
+            // The replay, in the reference's order (setup_optimization_info
+            // appends to vectors the reference never clears).
+            for (const auto &vec : candidates) {
+                copy_adj_mat_from(vec, src);
+                setup_optimization_info(use_in_exclusion_optimize);
+            }
+            // Orders that give the same ordered adjacency have the same
+            // restriction sets, IEP depth and scores.
+            {
+                std::map<uint64_t, int> first;
+                Schedule_IEP w;
+                w.alloc(n);
+                ns->rep.resize(candidates.size());
+                for (size_t c = 0; c < candidates.size(); ++c) {
+                    w.copy_adj_mat_from(candidates[c], src);
+                    ns->rep[c] = first.emplace(adj_key(w.adj_mat.data(), n), static_cast<int>(c)).first->second;
+                }
+            }
+            ns->candidates = std::move(candidates);
+            ns->replayed.reset(new Schedule_IEP(*this));
+            st = model_cache_insert(key, std::move(ns));
+        }
+        // Scores, in parallel; the minimum is taken in the reference's order
+        // (the first of equal scores wins).
+        const auto &cands = st->candidates;
+        std::vector<std::vector<double>> costs(cands.size());
 #pragma omp parallel
         {
             Schedule_IEP w;
             w.alloc(n);
-#pragma omp for schedule(dynamic, 1)
-            for (size_t c = 0; c < candidates.size(); ++c) {
-                w.copy_adj_mat_from(candidates[c], src);
-                w.setup_optimization_info(use_in_exclusion_optimize);
-                Eval &ev = evals[c];
-                w.restricts_generate(ev.sets);
-                if (ev.sets.empty()) {
-                    ev.costs.push_back(w.new_estimate_schedule_restrict(Pairs(), v_cnt, e_cnt, tri_cnt));
+#pragma omp for schedule(dynamic, 8)
+            for (size_t c = 0; c < cands.size(); ++c) {
+                if (st->rep[c] != static_cast<int>(c)) continue;
+                w.copy_adj_mat_from(cands[c], src);
+                w.in_exclusion_optimize_num = st->iep_num[c];
+                if (st->sets[c].empty()) {
+                    costs[c].push_back(w.new_estimate_schedule_restrict(Pairs(), v_cnt, e_cnt, tri_cnt));
                 } else {
-                    for (const auto &pairs : ev.sets)
-                        ev.costs.push_back(w.new_estimate_schedule_restrict(pairs, v_cnt, e_cnt, tri_cnt));
+                    for (const auto &pairs : st->sets[c])
+                        costs[c].push_back(w.new_estimate_schedule_restrict(pairs, v_cnt, e_cnt, tri_cnt));
                 }
             }
         }
-        for (size_t c = 0; c < candidates.size(); ++c) {
-            const auto &vec = candidates[c];
-            copy_adj_mat_from(vec, src);
-            setup_optimization_info(use_in_exclusion_optimize);
-            const Eval &ev = evals[c];
-            if (ev.sets.empty()) {
-                const double val = ev.costs[0];
-                if (!have_best || val < min_val) {
+        std::vector<int> best_order(n, 0);
+        double min_val = 1e18;
+        bool have_best = false;
+        for (size_t c = 0; c < cands.size(); ++c) {
+            const auto &sets = st->sets[c];
+            const std::vector<double> &cost = costs[st->rep[c]];
+            if (sets.empty()) {
+                if (!have_best || cost[0] < min_val) {
                     have_best = true;
-                    min_val = val;
-                    best_order = vec;
+                    min_val = cost[0];
+                    best_order = cands[c];
                     best_pairs.clear();
+                    best_ck = {static_cast<int>(c), -1};
                 }
             }
-            for (size_t k = 0; k < ev.sets.size(); ++k) {
-                const double val = ev.costs[k];
-                if (!have_best || val < min_val) {
+            for (size_t k = 0; k < sets.size(); ++k) {
+                if (!have_best || cost[k] < min_val) {
                     have_best = true;
-                    min_val = val;
-                    best_order = vec;
-                    best_pairs = ev.sets[k];
+                    min_val = cost[k];
+                    best_order = cands[c];
+                    best_pairs = sets[k];
+                    best_ck = {static_cast<int>(c), static_cast<int>(k)};
                 }
             }
         }
@@ -381,7 +475,23 @@ Schedule_IEP::Schedule_IEP(const Pattern &pattern, bool &is_pattern_valid, int p
     setup_optimization_info(use_in_exclusion_optimize);
     chosen_pairs_ = best_pairs;
     if (restricts_type != 0) add_restrict(best_pairs);
+    if (!st) {
+        set_in_exclusion_optimize_redundancy();
+        return;
+    }
+    // The redundancy depends on the pattern's replayed state and the chosen
+    // (order, restriction set) only.
+    {
+        std::lock_guard<std::mutex> lock(st->mu);
+        auto it = st->redundancy.find(best_ck);
+        if (it != st->redundancy.end()) {
+            in_exclusion_optimize_redundancy = it->second;
+            return;
+        }
+    }
     set_in_exclusion_optimize_redundancy();
+    std::lock_guard<std::mutex> lock(st->mu);
+    st->redundancy.emplace(best_ck, in_exclusion_optimize_redundancy);
 }
 
 Schedule_IEP::Schedule_IEP(const Pattern &pattern, const std::vector<int> &order, const Pairs &restricts,
@@ -634,14 +744,46 @@ void Schedule_IEP::add_restrict(const Pairs &restricts) {
     }
 }
 
+// The permutations v with adj(i, j) => adj(v[i], v[j]) (the automorphisms),
+// in lexicographic order like a scan of all n! permutations: positions are
+// filled in turn with the smallest unused vertex of the same degree whose
+// edges to the earlier positions are kept.
 std::vector<std::vector<int>> Schedule_IEP::get_isomorphism_vec() const {
     std::vector<std::vector<int>> out;
-    for (const auto &v : all_permutations(size)) {
-        bool ok = true;
-        for (int i = 0; i < size && ok; ++i)
-            for (int j = i + 1; j < size; ++j)
-                if (adj_mat[i * size + j] && !adj_mat[v[i] * size + v[j]]) { ok = false; break; }
-        if (ok) out.push_back(v);
+    const int n = size;
+    int deg[kMaxPatternSize] = {};
+    for (int i = 0; i < n; ++i)
+        for (int j = 0; j < n; ++j) deg[i] += adj_mat[i * n + j] != 0;
+    std::vector<int> v(n, -1);
+    bool used[kMaxPatternSize] = {};
+    int cand[kMaxPatternSize + 1];  // next vertex to try at each position
+    int i = 0;
+    cand[0] = 0;
+    while (i >= 0) {
+        if (i == n) {
+            out.push_back(v);
+            --i;
+            used[v[i]] = false;
+            continue;
+        }
+        int x = cand[i];
+        for (; x < n; ++x) {
+            if (used[x] || deg[x] != deg[i]) continue;
+            bool ok = true;
+            for (int j = 0; j < i && ok; ++j)
+                if (adj_mat[j * n + i] && !adj_mat[v[j] * n + x]) ok = false;
+            if (ok) break;
+        }
+        if (x == n) {  // position i exhausted: back to i - 1
+            --i;
+            if (i >= 0) used[v[i]] = false;
+            continue;
+        }
+        v[i] = x;
+        used[x] = true;
+        cand[i] = x + 1;
+        ++i;
+        if (i < n) cand[i] = 0;
     }
     return out;
 }
@@ -853,12 +995,6 @@ struct CompleteDfs {
         sets.resize(std::max(1, s.get_total_prefix_num()));
         ans_buf.resize(s.in_exclusion_optimize_vertex_id.size() + 1);
     }
-    std::vector<int> nbrs(int v) const {
-        std::vector<int> r;
-        for (int u = 0; u < kn; ++u)
-            if (u != v) r.push_back(u);
-        return r;
-    }
     bool has(int v) const { return std::find(emb.begin(), emb.end(), v) != emb.end(); }
     int subtract_size(const std::vector<int> &set0, int size0) const {
         int ret = size0;
@@ -866,15 +1002,19 @@ struct CompleteDfs {
             if (std::binary_search(set0.begin(), set0.begin() + size0, x)) --ret;
         return ret;
     }
+    // S_p = S_father ∩ N(v); in K_kn, N(v) is every vertex but v, so the
+    // intersection is the father's set without v (all vertices but v for a
+    // prefix without father).
     void build(int p, int v) {
         const int f = s.get_father_prefix_id(p);
-        std::vector<int> nb = nbrs(v);
+        std::vector<int> &out = sets[p];
+        out.clear();
         if (f == -1) {
-            sets[p] = nb;
+            for (int u = 0; u < kn; ++u)
+                if (u != v) out.push_back(u);
         } else {
-            std::vector<int> out;
-            std::set_intersection(sets[f].begin(), sets[f].end(), nb.begin(), nb.end(), std::back_inserter(out));
-            sets[p] = out;
+            for (int u : sets[f])
+                if (u != v) out.push_back(u);
         }
     }
     void run() {
@@ -972,6 +1112,15 @@ bool Schedule_IEP::iep_tables_out_of_range() const {
 }
 
 long long Schedule_IEP::count_on_complete_graph(int kn) const {
+    if (is_vertex_induced) {
+        // Every vertex of K_kn is adjacent to every other, so the
+        // vertex-induced filter keeps, at a position with a non-adjacent
+        // earlier position u, only the vertex already matched to u: the
+        // count of a pattern that is not complete is 0.
+        for (int i = 0; i < size; ++i)
+            for (int j = i + 1; j < size; ++j)
+                if (!adj_mat[i * size + j]) return 0;
+    }
     CompleteDfs d(*this, kn);
     d.run();
     return d.ans / in_exclusion_optimize_redundancy;

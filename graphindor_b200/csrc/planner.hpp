@@ -11,6 +11,7 @@
 #pragma once
 
 #include <cstdint>
+#include <memory>
 #include <stdexcept>
 #include <string>
 #include <utility>
@@ -76,9 +77,6 @@ public:
     // Vertex-induced plan with the pattern's own order and no restrictions
     // (reference src/schedule_IEP.cpp:249-290).
     Schedule_IEP(const int *adj_mat, int size);
-
-    Schedule_IEP(const Schedule_IEP &) = delete;
-    Schedule_IEP &operator=(const Schedule_IEP &) = delete;
 
     int get_size() const { return size; }
     int get_total_prefix_num() const { return total_prefix_num; }
@@ -162,6 +160,10 @@ public:
 
 private:
     Schedule_IEP() = default;
+    // Not copyable from outside, as in the reference (schedule_IEP.h:27-28);
+    // the model constructor copies the state it caches per pattern.
+    Schedule_IEP(const Schedule_IEP &) = default;
+    Schedule_IEP &operator=(const Schedule_IEP &) = default;
     void alloc(int n);
     bool check_connectivity() const;
     int get_max_degree() const;
@@ -174,6 +176,14 @@ private:
     void restricts_generate(std::vector<std::vector<std::pair<int, int>>> &out) const;
     void set_in_exclusion_optimize_redundancy();
     std::vector<std::vector<int>> get_isomorphism_vec() const;
+
+public:
+    struct ModelKey;
+    struct ModelState;
+
+private:
+    static std::shared_ptr<const ModelState> model_cache_find(const ModelKey &k);
+    static std::shared_ptr<const ModelState> model_cache_insert(const ModelKey &k, std::shared_ptr<ModelState> s);
 
     int size = 0;
     std::vector<int> adj_mat;

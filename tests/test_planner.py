@@ -51,7 +51,25 @@ def _out_of_range(ref) -> bool:
 
 @pytest.mark.parametrize("idx", range(len(JOBS)), ids=[j["job"][:60] for j in JOBS])
 def test_plan_matches_reference(native, idx):
-    job, ref = JOBS[idx]["job"], JOBS[idx]["ref"]
+    check_plan(JOBS[idx]["job"], JOBS[idx]["ref"])
+
+
+def test_plans_do_not_depend_on_planning_order(native):
+    """The planner keeps each pattern's graph-independent state and rescores
+    it for the next graph.  Planning every golden job in reverse order in a
+    fresh process (so another graph's plan fills that state first) gives the
+    same plans."""
+    import subprocess
+    import sys
+    from pathlib import Path
+    here = Path(__file__).resolve().parent
+    code = ("import sys; sys.path[:0] = [%r, %r]; import test_planner as t\n"
+            "for j in reversed(t.JOBS): t.check_plan(j['job'], j['ref'])\n" % (str(here), str(here.parent)))
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=900)
+    assert r.returncode == 0, r.stderr[-2000:]
+
+
+def check_plan(job: str, ref: dict) -> None:
     mine = _plan(job).export()
     if _out_of_range(ref):
         # Same order and restrictions; clean IEP tables instead of the
