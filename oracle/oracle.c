@@ -701,20 +701,40 @@ static void pivot_rec(pivot_t *t, int64_t depth, int h, int64_t q) {
     const int64_t W = t->W;
     const uint64_t *S = t->cand + depth * W;
     const int K1 = t->kmax + 1;
-    if (h >= t->kmax - 2) {
+    if (h >= t->kmax - 3) {
         /* The subtree of this node counts every clique R ∪ P' ∪ C once, R the
          * h required vertices, P' a subset of the q optional ones and C a
-         * clique of G[S].  With at most two vertices left to add up to kmax,
-         * the k-clique count is sum_j C(q, j) cl(k - h - j), where cl(0) = 1,
-         * cl(1) = |S| and cl(2) = the edges of G[S]; no descent needed. */
-        uint64_t cl[3] = {1, 0, 0};
+         * clique of G[S].  With at most three vertices left to add up to
+         * kmax, the k-clique count is sum_j C(q, j) cl(k - h - j), where
+         * cl(0) = 1, cl(1) = |S|, cl(2) = the edges and cl(3) = the
+         * triangles of G[S]; no descent needed. */
+        uint64_t cl[4] = {1, 0, 0, 0};
         for (int64_t w = 0; w < W; ++w) cl[1] += (uint64_t)__builtin_popcountll(S[w]);
-        if (h == t->kmax - 2) {
-            uint64_t twice = 0;
+        if (h <= t->kmax - 2) {
+            uint64_t *R = t->rest + depth * W; /* free: this node has no children */
+            uint64_t twice = 0, tri = 0;
             for (int64_t w = 0; w < W; ++w)
-                for (uint64_t b = S[w]; b; b &= b - 1)
-                    twice += (uint64_t)row_popcount_and(S, t->adj + (w * 64 + __builtin_ctzll(b)) * W, W);
+                for (uint64_t b = S[w]; b; b &= b - 1) {
+                    const int64_t x = w * 64 + __builtin_ctzll(b);
+                    const uint64_t *ax = t->adj + x * W;
+                    twice += (uint64_t)row_popcount_and(S, ax, W);
+                    if (h > t->kmax - 3) continue;
+                    /* triangles x < y < z: R = S ∩ N(x) above x, then
+                     * |R ∩ N(y)| above y for each y in R */
+                    for (int64_t i = 0; i < W; ++i) R[i] = i < w ? 0 : S[i] & ax[i];
+                    R[w] &= x % 64 == 63 ? 0 : ~((2ull << (x % 64)) - 1);
+                    for (int64_t wy = w; wy < W; ++wy)
+                        for (uint64_t by = R[wy]; by; by &= by - 1) {
+                            const int64_t y = wy * 64 + __builtin_ctzll(by);
+                            const uint64_t *ay = t->adj + y * W;
+                            uint64_t c = (uint64_t)__builtin_popcountll(
+                                R[wy] & ay[wy] & (y % 64 == 63 ? 0 : ~((2ull << (y % 64)) - 1)));
+                            for (int64_t i = wy + 1; i < W; ++i) c += (uint64_t)__builtin_popcountll(R[i] & ay[i]);
+                            tri += c;
+                        }
+                }
             cl[2] = twice / 2;
+            cl[3] = tri;
         }
         for (int k = h; k <= t->kmax; ++k)
             for (int j = 0; j <= k - h && j <= q; ++j) t->acc[k] += t->binom[q * K1 + j] * cl[k - h - j];

@@ -74,9 +74,10 @@ uint64_t oracle_clique_count(int k, const int64_t *vertex, const int32_t *edge, 
  * and has one child S ∩ N(u) in which u is optional, and one child per other
  * w ∈ S \ N(u), S ∩ N(w) minus the earlier such w, in which w is required.
  * A leaf with h required and q optional vertices holds C(q, k - h)
- * k-cliques.  A node two or fewer vertices short of kmax is counted in
- * closed form from its candidates' number and induced edges (no descent),
- * so the search never goes below h = kmax - 2.  Each root's candidates
+ * k-cliques.  A node three or fewer vertices short of kmax is counted in
+ * closed form from its candidates' number, induced edges and induced
+ * triangles (no descent), so the search never goes below h = kmax - 3.
+ * Each root's candidates
  * and their induced adjacency are bit rows of ceil(|N+(v)| / 64) words.  An
  * independent check of the engine's k-clique counts for large k, where
  * enumeration is too slow.  Returns 0, or -1 on bad input or no memory. */
