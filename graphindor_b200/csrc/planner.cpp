@@ -16,6 +16,7 @@
 #include <mutex>
 #include <numeric>
 #include <tuple>
+#include <unordered_map>
 
 namespace gi {
 
@@ -118,6 +119,33 @@ uint64_t adj_key(const int *adj, int n) {
 
 using Pairs = std::vector<std::pair<int, int>>;
 
+// A restriction list of up to 20 pairs over positions < 8, packed 6 bits a
+// pair (a * 8 + b + 1, never 0) into two words, with a tag word: a hash key
+// for the planner's memo tables.
+struct PackedKey {
+    uint64_t tag, w0, w1;
+    bool operator==(const PackedKey &o) const { return tag == o.tag && w0 == o.w0 && w1 == o.w1; }
+};
+struct PackedKeyHash {
+    size_t operator()(const PackedKey &k) const {
+        uint64_t h = k.tag * 0x9E3779B97F4A7C15ull;
+        h ^= k.w0 + 0x9E3779B97F4A7C15ull + (h << 6) + (h >> 2);
+        h ^= k.w1 + 0x9E3779B97F4A7C15ull + (h << 6) + (h >> 2);
+        return static_cast<size_t>(h);
+    }
+};
+bool pack_pairs(uint64_t tag, const Pairs &r, PackedKey &out) {
+    if (r.size() > 20) return false;
+    out = {tag, 0, 0};
+    for (size_t i = 0; i < r.size(); ++i) {
+        const auto &p = r[i];
+        if (p.first < 0 || p.first >= 8 || p.second < 0 || p.second >= 8) return false;
+        const uint64_t v = static_cast<uint64_t>(p.first * 8 + p.second + 1);
+        (i < 10 ? out.w0 : out.w1) |= v << (6 * (i % 10));
+    }
+    return true;
+}
+
 // Depth-first search of restriction sets (reference
 // src/schedule_IEP.cpp:785-840).
 void restriction_dfs(const Pattern &base_dag, std::vector<std::vector<int>> iso,
@@ -161,10 +189,17 @@ void restriction_dfs(const Pattern &base_dag, std::vector<std::vector<int>> iso,
 // restriction list, turned into conditional selectivities (reference
 // src/schedule_IEP.cpp:330-346).  Memoised per thread.
 const std::vector<double> &restriction_selectivity(const Pairs &sorted, int n) {
-    thread_local std::map<std::pair<int, Pairs>, std::vector<double>> cache;
-    auto key = std::make_pair(n, sorted);
-    auto it = cache.find(key);
-    if (it != cache.end()) return it->second;
+    thread_local std::unordered_map<PackedKey, std::vector<double>, PackedKeyHash> cache;
+    thread_local std::map<std::pair<int, Pairs>, std::vector<double>> long_cache;  // lists that do not pack
+    PackedKey key;
+    const bool packed = pack_pairs(static_cast<uint64_t>(n), sorted, key);
+    if (packed) {
+        auto it = cache.find(key);
+        if (it != cache.end()) return it->second;
+    } else {
+        auto it = long_cache.find(std::make_pair(n, sorted));
+        if (it != long_cache.end()) return it->second;
+    }
     const int rs = static_cast<int>(sorted.size());
     std::vector<double> sum(rs, 0.0);
     std::vector<int> tmp(n);
@@ -181,7 +216,8 @@ const std::vector<double> &restriction_selectivity(const Pairs &sorted, int n) {
     for (int i = 2; i <= n; ++i) total *= i;
     for (int i = 0; i < rs; ++i) sum[i] = sum[i] / total;
     for (int i = rs - 1; i > 0; --i) sum[i] /= sum[i - 1];
-    return cache.emplace(key, std::move(sum)).first->second;
+    if (packed) return cache.emplace(key, std::move(sum)).first->second;
+    return long_cache.emplace(std::make_pair(n, sorted), std::move(sum)).first->second;
 }
 
 // Drops pairs implied by two others, as add_restrict does (reference
@@ -214,35 +250,67 @@ Pairs filter_implied(Pairs r) {
 // same for every ranking π (then count = raw / it), or 0 when it varies (R
 // over- or under-counts some subgraphs).  Memoised per thread.
 int restriction_multiplicity(const int *adj, int n, const std::vector<std::pair<int, int>> &R) {
-    thread_local std::map<std::pair<uint64_t, Pairs>, int> cache;
-    auto key = std::make_pair(adj_key(adj, n), R);
-    auto it = cache.find(key);
-    if (it != cache.end()) return it->second;
+    thread_local std::unordered_map<PackedKey, int, PackedKeyHash> cache;
+    PackedKey key;
+    const bool packed = pack_pairs(adj_key(adj, n), R, key);
+    if (packed) {
+        auto it = cache.find(key);
+        if (it != cache.end()) return it->second;
+    }
+    // Automorphisms by backtracking: position i takes an unused vertex of the
+    // same degree whose adjacency to the earlier positions matches.
     std::vector<std::vector<int>> aut;
-    for (const auto &p : all_permutations(n)) {
-        bool ok = true;
-        for (int i = 0; i < n && ok; ++i)
-            for (int j = 0; j < n; ++j)
-                if ((adj[i * n + j] != 0) != (adj[p[i] * n + p[j]] != 0)) { ok = false; break; }
-        if (ok) aut.push_back(p);
+    {
+        int deg[kMaxPatternSize] = {};
+        for (int i = 0; i < n; ++i)
+            for (int j = 0; j < n; ++j) deg[i] += adj[i * n + j] != 0;
+        std::vector<int> p(n);
+        bool used[kMaxPatternSize] = {};
+        auto extend = [&](auto &&self, int i) -> void {
+            if (i == n) {
+                aut.push_back(p);
+                return;
+            }
+            for (int x = 0; x < n; ++x) {
+                if (used[x] || deg[x] != deg[i]) continue;
+                bool ok = true;
+                for (int j = 0; j < i && ok; ++j) ok = (adj[j * n + i] != 0) == (adj[p[j] * n + x] != 0);
+                if (!ok) continue;
+                p[i] = x;
+                used[x] = true;
+                self(self, i + 1);
+                used[x] = false;
+            }
+        };
+        extend(extend, 0);
     }
     int common = -1;
-    for (const auto &pi : all_permutations(n)) {
-        int c = 0;
-        for (const auto &s : aut) {
-            bool sat = true;
-            for (const auto &r : R)
-                if (!(pi[s[r.second]] < pi[s[r.first]])) { sat = false; break; }
-            c += sat;
-        }
-        if (common == -1) common = c;
-        if (c != common || c == 0) {
-            common = 0;
-            break;
-        }
+    if (R.empty()) {
+        common = static_cast<int>(aut.size());  // every ranking satisfies no restriction
+    } else if (aut.size() == 1) {
+        common = 0;  // some ranking breaks a restriction: count 0 for it
     }
-    if (common < 0) common = 0;
-    cache.emplace(key, common);
+    if (common == -1) {
+        // c(pi) = automorphisms s whose ranking pi∘s satisfies R; it must be
+        // the same, and nonzero, for every ranking pi.
+        int first = -1;
+        for (const auto &pi : all_permutations(n)) {
+            int c = 0;
+            for (const auto &s : aut) {
+                bool sat = true;
+                for (const auto &r : R)
+                    if (!(pi[s[r.second]] < pi[s[r.first]])) { sat = false; break; }
+                c += sat;
+            }
+            if (first == -1) first = c;
+            if (c != first || c == 0) {
+                first = 0;
+                break;
+            }
+        }
+        common = first < 0 ? 0 : first;
+    }
+    if (packed) cache.emplace(key, common);
     return common;
 }
 
@@ -1132,44 +1200,92 @@ std::vector<Schedule_IEP::Candidate> Schedule_IEP::enumerate_candidates(const Pa
     std::vector<Candidate> out;
     const int n = pattern.get_size();
     if (n < 2 || n > kMaxPatternSize || !pattern.check_connected()) return out;
-    Schedule_IEP s;
-    s.alloc(n);
-    std::copy(pattern.get_adj_mat_ptr(), pattern.get_adj_mat_ptr() + n * n, s.adj_mat.begin());
-    auto candidates = all_permutations(n);
-    candidates.erase(std::remove_if(candidates.begin(), candidates.end(),
-                                    [&](const std::vector<int> &v) { return s.get_vec_optimize_num(v) < 0; }),
-                     candidates.end());
-    int max_val = 0;
-    for (const auto &v : candidates) max_val = std::max(max_val, s.get_vec_optimize_num(v));
-    candidates.erase(std::remove_if(candidates.begin(), candidates.end(),
-                                    [&](const std::vector<int> &v) { return s.get_vec_optimize_num(v) != max_val; }),
-                     candidates.end());
-    // Orders are independent: evaluated in parallel on per-thread copies,
-    // concatenated in order.
-    std::vector<std::vector<Candidate>> per(candidates.size());
+    const int *src = pattern.get_adj_mat_ptr();
+    // The candidates without their scores depend on the pattern alone and
+    // are kept per pattern (bounded like the model constructor's state);
+    // score_of[i] is the first candidate with candidate i's ordered
+    // adjacency and restriction set, whose score it shares.
+    struct EnumState {
+        std::vector<Candidate> cands;
+        std::vector<int> score_of;
+    };
+    static std::mutex mu;
+    static std::map<std::pair<uint64_t, bool>, std::shared_ptr<const EnumState>> cache;
+    const auto key = std::make_pair(adj_key(src, n), use_iep);
+    std::shared_ptr<const EnumState> st;
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        auto it = cache.find(key);
+        if (it != cache.end()) st = it->second;
+    }
+    if (!st) {
+        Schedule_IEP s;
+        s.alloc(n);
+        std::copy(src, src + n * n, s.adj_mat.begin());
+        auto candidates = all_permutations(n);
+        candidates.erase(std::remove_if(candidates.begin(), candidates.end(),
+                                        [&](const std::vector<int> &v) { return s.get_vec_optimize_num(v) < 0; }),
+                         candidates.end());
+        int max_val = 0;
+        for (const auto &v : candidates) max_val = std::max(max_val, s.get_vec_optimize_num(v));
+        candidates.erase(std::remove_if(candidates.begin(), candidates.end(),
+                                        [&](const std::vector<int> &v) {
+                                            return s.get_vec_optimize_num(v) != max_val;
+                                        }),
+                         candidates.end());
+        // Orders are independent: evaluated in parallel on per-thread copies,
+        // concatenated in order.
+        std::vector<std::vector<Candidate>> per(candidates.size());
+        std::vector<uint64_t> okey(candidates.size());
+#pragma omp parallel
+        {
+            Schedule_IEP w;
+            w.alloc(n);
+#pragma omp for schedule(dynamic, 1)
+            for (size_t c = 0; c < candidates.size(); ++c) {
+                const auto &vec = candidates[c];
+                w.copy_adj_mat_from(vec, src);
+                okey[c] = adj_key(w.adj_mat.data(), n);
+                w.setup_optimization_info(use_iep);
+                std::vector<Pairs> rv;
+                w.restricts_generate(rv);
+                if (rv.empty()) rv.push_back(Pairs());
+                for (const auto &pairs : rv) {
+                    std::vector<std::pair<int, int>> applied;
+                    for (const auto &p : filter_implied(pairs))
+                        if (p.second < n - w.in_exclusion_optimize_num) applied.push_back(p);
+                    const int div = restriction_multiplicity(w.adj_mat.data(), n, applied);
+                    per[c].push_back({vec, pairs, 0.0, div, w.in_exclusion_optimize_num});
+                }
+            }
+        }
+        auto ns = std::make_shared<EnumState>();
+        std::map<std::pair<uint64_t, size_t>, int> first;
+        for (size_t c = 0; c < per.size(); ++c)
+            for (size_t k = 0; k < per[c].size(); ++k) {
+                const int i = static_cast<int>(ns->cands.size());
+                ns->score_of.push_back(first.emplace(std::make_pair(okey[c], k), i).first->second);
+                ns->cands.push_back(std::move(per[c][k]));
+            }
+        std::lock_guard<std::mutex> lock(mu);
+        if (cache.size() >= 4096) cache.clear();
+        st = cache.emplace(key, std::move(ns)).first->second;
+    }
+    out = st->cands;
+    const int total = static_cast<int>(out.size());
 #pragma omp parallel
     {
         Schedule_IEP w;
         w.alloc(n);
-#pragma omp for schedule(dynamic, 1)
-        for (size_t c = 0; c < candidates.size(); ++c) {
-            const auto &vec = candidates[c];
-            w.copy_adj_mat_from(vec, pattern.get_adj_mat_ptr());
-            w.setup_optimization_info(use_iep);
-            std::vector<Pairs> rv;
-            w.restricts_generate(rv);
-            if (rv.empty()) rv.push_back(Pairs());
-            for (const auto &pairs : rv) {
-                std::vector<std::pair<int, int>> applied;
-                for (const auto &p : filter_implied(pairs))
-                    if (p.second < n - w.in_exclusion_optimize_num) applied.push_back(p);
-                const int div = restriction_multiplicity(w.adj_mat.data(), n, applied);
-                per[c].push_back({vec, pairs, w.new_estimate_schedule_restrict(pairs, v_cnt, e_cnt, tri_cnt), div,
-                                  w.in_exclusion_optimize_num});
-            }
+#pragma omp for schedule(dynamic, 8)
+        for (int i = 0; i < total; ++i) {
+            if (st->score_of[i] != i) continue;
+            w.copy_adj_mat_from(out[i].order, src);
+            w.in_exclusion_optimize_num = out[i].iep_k;
+            out[i].model_cost = w.new_estimate_schedule_restrict(out[i].restricts, v_cnt, e_cnt, tri_cnt);
         }
     }
-    for (auto &v : per) out.insert(out.end(), v.begin(), v.end());
+    for (int i = 0; i < total; ++i) out[i].model_cost = out[st->score_of[i]].model_cost;
     return out;
 }
 

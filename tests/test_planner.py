@@ -90,3 +90,28 @@ def check_plan(job: str, ref: dict) -> None:
 def test_out_of_range_cases_exist_and_are_rare():
     bad = sum(_out_of_range(j["ref"]) for j in JOBS)
     assert 0 < bad < len(JOBS) // 10
+
+
+def test_candidates_do_not_depend_on_planning_order(native):
+    """Candidate lists keep their pattern-only part per pattern and rescore
+    it per graph: a list computed after another graph's equals the one a fresh
+    process computes first (orders, restrictions, costs bit for bit, divisors)."""
+    import subprocess
+    import sys
+    from pathlib import Path
+    graphs = [(4194304, 85916670, 7515023), (7115, 201524, 608389), (1000, 32000, 5000)]
+    pats = [(5, "0101110101010101010011000"), (6, "011100101010110001100011010101001110"),
+            (6, "010101101000010100101010000101100010"), (7, "0111111101111111011111110111111101111111011111110")]
+    code = ("import sys, json; sys.path[:0] = [%r]; import graphindor_b200 as gi\n"
+            "g = json.loads(sys.argv[1]); out = []\n"
+            "for n, a in json.loads(sys.argv[2]):\n"
+            "    out.append([[o, r, c.hex(), d] for o, r, c, d in gi.Schedule_IEP.candidates(gi.Pattern(n, a), *g)])\n"
+            "print(json.dumps(out))\n" % str(Path(__file__).resolve().parent.parent))
+    import json
+    for g in graphs:  # this process: every graph in turn, so later graphs hit the kept state
+        mine = [[[o, [list(p) for p in r], c.hex(), d] for o, r, c, d in gi.Schedule_IEP.candidates(gi.Pattern(n, a), *g)]
+                for n, a in pats]
+        r = subprocess.run([sys.executable, "-c", code, json.dumps(g), json.dumps(pats)], capture_output=True,
+                           text=True, timeout=600)
+        assert r.returncode == 0, r.stderr[-2000:]
+        assert mine == json.loads(r.stdout), g
