@@ -173,18 +173,30 @@ int gi_plan_create_learned(int n, const char *adj, int32_t v_cnt, int64_t e_cnt,
         Pattern pat(n, adj);
         if (!pat.check_connected()) return fail(GI_EDISCONNECTED, "pattern is not connected");
         const auto cands = Schedule_IEP::enumerate_candidates(pat, enable_iep != 0, v_cnt, e_cnt, tri_cnt);
-        std::vector<float> x(kDim);
-        std::memcpy(x.data() + kPlanDim, graph_features, sizeof(float) * kGraphDim);
+        // Predictions of the valid candidates, in parallel (each one computed
+        // the same way on any thread); the minimum is taken in candidate
+        // order, the first of equal predictions winning.
+        const int64_t nc = static_cast<int64_t>(cands.size());
+        std::vector<float> y(static_cast<size_t>(nc), 0.f);
+#pragma omp parallel
+        {
+            std::vector<float> x(kDim);
+            std::memcpy(x.data() + kPlanDim, graph_features, sizeof(float) * kGraphDim);
+#pragma omp for schedule(dynamic, 16)
+            for (int64_t i = 0; i < nc; ++i) {
+                const auto &c = cands[static_cast<size_t>(i)];
+                if (c.divisor <= 0) continue;
+                plan_features(n, pat.get_adj_mat_ptr(), c.order, c.restricts, c.model_cost, c.iep_k, x.data());
+                y[static_cast<size_t>(i)] = forward(m, x.data());
+            }
+        }
         int best = -1;
         float best_y = 0.f;
-        for (size_t i = 0; i < cands.size(); ++i) {
-            const auto &c = cands[i];
-            if (c.divisor <= 0) continue;
-            plan_features(n, pat.get_adj_mat_ptr(), c.order, c.restricts, c.model_cost, c.iep_k, x.data());
-            const float y = forward(m, x.data());
-            if (best < 0 || y < best_y) {
+        for (int64_t i = 0; i < nc; ++i) {
+            if (cands[static_cast<size_t>(i)].divisor <= 0) continue;
+            if (best < 0 || y[static_cast<size_t>(i)] < best_y) {
                 best = static_cast<int>(i);
-                best_y = y;
+                best_y = y[static_cast<size_t>(i)];
             }
         }
         if (best < 0) return fail(GI_EINVAL, "pattern has no valid candidate schedule");
