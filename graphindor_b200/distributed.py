@@ -1,13 +1,17 @@
-"""One count across the ranks of a torch.distributed process group, one GPU
-per rank (reference gpu/gpu_graph_static_task.cu, gpu/gpu_graph_mpi.cu).
+"""Counts across the ranks of a torch.distributed process group, one GPU per
+rank (reference gpu/gpu_graph_static_task.cu, gpu/gpu_graph_mpi.cu).
 
-Every rank holds a replica of the graph on its own GPU and counts its shard of
-the first-level work with ``gi_count_shard`` (chunk c belongs to shard
+``count``: every rank holds a replica of the graph on its own GPU and counts
+its shard of the first-level work with ``gi_count_shard`` (chunk c belongs to shard
 c mod world, the reference's static interleave,
 gpu/src/gpu_pattern_matching_static_task.cuh:63).  The only exchange is one
 all-reduce of the raw sums, added modulo 2^64 as the reference's GPU sum is;
 the total is divided by the plan's count divisor once, as a single-GPU count
 divides its whole sum (reference gpu/gpu_graph.cu:42-44).
+
+``batch_counts``: many (graph, pattern) jobs are spread over the ranks by
+their analytic cost; each rank counts its own jobs in one batched launch and
+one all-reduce of the per-job counts gives every rank all of them.
 """
 from __future__ import annotations
 
@@ -65,3 +69,54 @@ def divisor(schedule) -> int:
     d = N.PlanDesc()
     check(lib().gi_plan_export(schedule.handle, C.byref(d)), "gi_plan_export")
     return int(d.count_divisor)
+
+
+def assign_jobs(costs: Sequence[float], world: int) -> list[int]:
+    """Owner rank of each job: longest first onto the least-loaded rank
+    (ties to the lower job index and the lower rank), so every rank computes
+    the same assignment from the same costs."""
+    if world < 1:
+        raise ValueError("world must be >= 1")
+    order = sorted(range(len(costs)), key=lambda j: (-float(costs[j]), j))
+    load = [0.0] * world
+    owner = [0] * len(costs)
+    for j in order:
+        r = min(range(world), key=lambda x: (load[x], x))
+        owner[j] = r
+        load[r] += max(float(costs[j]), 0.0)
+    return owner
+
+
+def batch_counts(jobs: Sequence, group=None, *, costs: Optional[Sequence[float]] = None,
+                 runner: Optional[Callable[[list], Sequence[int]]] = None) -> list[int]:
+    """Counts of many (graph, schedule) jobs spread over the group's ranks,
+    one GPU each.  Every rank passes the same job list (its own graph
+    handles, on its own GPU), runs the jobs ``assign_jobs`` gives it as one
+    batch (``graphindor_b200.Batch``), and one all-reduce of the counts (0
+    where another rank owns the job) hands every rank all of them.  ``costs``
+    orders the assignment (default: each schedule's analytic model cost);
+    ``runner(local_jobs) -> counts`` replaces the batch (a CPU stand-in lets
+    the exchange run on hosts without GPUs)."""
+    import torch.distributed as dist
+
+    rank, world = dist.get_rank(group), dist.get_world_size(group)
+    if costs is None:
+        costs = [s.export()["model_cost"] for _, s in jobs]
+    if len(costs) != len(jobs):
+        raise ValueError("one cost per job")
+    owner = assign_jobs(costs, world)
+    mine = [j for j in range(len(jobs)) if owner[j] == rank]
+    local: Sequence[int] = []
+    if mine:
+        local_jobs = [jobs[j] for j in mine]
+        if runner is not None:
+            local = runner(local_jobs)
+        else:
+            from . import Batch
+            local = Batch(local_jobs).run()[0]
+        if len(local) != len(mine):
+            raise RuntimeError("the runner returned the wrong number of counts")
+    values = [0] * len(jobs)
+    for j, c in zip(mine, local):
+        values[j] = int(c)
+    return allreduce_u64(values, group)

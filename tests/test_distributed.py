@@ -1,8 +1,8 @@
 """The multi-rank path on CPU: world-size-2 gloo process groups run the
-exchange of graphindor_b200.distributed with the oracle standing in for each
-rank's GPU shard count (vertex-strided shards), and check the total against
-the single-process count; the modulo-2^64 reduction; and a rank that fails
-before the exchange."""
+exchanges of graphindor_b200.distributed with the oracle standing in for each
+rank's GPU work (vertex-strided shards of one count; the jobs of a batch),
+and check the results against single-process counts; the modulo-2^64
+reduction; the job assignment; and a rank that fails before the exchange."""
 from __future__ import annotations
 
 import datetime
@@ -52,6 +52,65 @@ def _count_worker(rank, world, port, q):
         q.put((rank, out, wrap))
     except Exception as e:  # reported to the parent
         q.put((rank, "error", repr(e)))
+
+
+def _batch_worker(rank, world, port, q):
+    sys.path[:0] = [str(ROOT), str(ROOT / "oracle"), str(ROOT / "tests")]
+    try:
+        import torch.distributed as dist
+        import graphindor_b200 as gi
+        from graphindor_b200 import distributed as gd, gen
+        import oracle_py
+        from conftest import plan_desc
+        _init(rank, world, port)
+        jobs = _batch_jobs(gi, gen)
+        ran = []
+
+        def runner(local):
+            ran.extend(id(j) for j in local)
+            return [oracle_py.count(plan_desc(s), g.vertex, g.edge)[0] // plan_desc(s).count_divisor
+                    for g, s in local]
+        counts = gd.batch_counts(jobs, runner=runner)
+        mine = sorted(i for i, j in enumerate(jobs) if id(j) in ran)
+        dist.destroy_process_group()
+        q.put((rank, counts, mine))
+    except Exception as e:  # reported to the parent
+        q.put((rank, "error", repr(e)))
+
+
+def _batch_jobs(gi, gen):
+    graphs = [gen.rmat(9, 8.0, 21), gen.rmat(10, 6.0, 22), gen.erdos_renyi(600, 5000, 23)]
+    pats = [(3, "011101110"), (4, "0110100110010110"), (4, "0111101111001100"), (5, "0101110101010101010011000")]
+    return [(g, gi.Schedule_IEP(gi.Pattern(n, a), g.v_cnt, g.e_cnt, 0)) for g in graphs for n, a in pats]
+
+
+def test_batch_jobs_spread_over_two_ranks(oracle, native):
+    """Each rank counts only the jobs assigned to it, the two sets cover all
+    jobs once, and both ranks end with every job's count."""
+    import graphindor_b200 as gi
+    from graphindor_b200 import gen
+    from conftest import plan_desc
+    res = _run(_batch_worker)
+    jobs = _batch_jobs(gi, gen)
+    want = [oracle.count(plan_desc(s), g.vertex, g.edge)[0] // plan_desc(s).count_divisor for g, s in jobs]
+    for rank, counts, mine in res:
+        assert counts != "error", mine
+        assert counts == want
+    assert sorted(res[0][2] + res[1][2]) == list(range(len(jobs)))
+    assert res[0][2] and res[1][2]
+
+
+def test_job_assignment_is_balanced_and_deterministic():
+    from graphindor_b200.distributed import assign_jobs
+    costs = [9.0, 1.0, 8.0, 2.0, 7.0, 3.0, 6.0, 4.0, 5.0, 0.0]
+    owner = assign_jobs(costs, 3)
+    assert owner == assign_jobs(list(costs), 3)
+    load = [sum(c for c, o in zip(costs, owner) if o == r) for r in range(3)]
+    assert max(load) - min(load) <= max(costs)
+    assert assign_jobs(costs, 1) == [0] * len(costs)
+    assert assign_jobs([], 4) == []
+    with pytest.raises(ValueError):
+        assign_jobs(costs, 0)
 
 
 def _fail_worker(rank, world, port, q):

@@ -207,7 +207,8 @@ def test_edge_cases(oracle):
 
 
 def test_distributed_count_over_nccl_matches_the_single_gpu_count(golden_graphs, dev_graphs):
-    """World size 1 over NCCL: the shard count plus the 2^64 all-reduce."""
+    """World size 1 over NCCL: the shard count plus the 2^64 all-reduce, and a
+    batch whose jobs are spread over the ranks."""
     import datetime
     import os
     import socket
@@ -226,6 +227,10 @@ def test_distributed_count_over_nccl_matches_the_single_gpu_count(golden_graphs,
             s = gi.Schedule_IEP(gi.Pattern(n, adj), g.v_cnt, g.e_cnt, 0)
             assert gd.count(dg, s) == gi.pattern_matching(dg, s).count
         assert gd.allreduce_u64([(1 << 64) - 1]) == [(1 << 64) - 1]
+        # Jobs of a batch spread over the ranks (here one) and exchanged.
+        jobs = [(dg, gi.Schedule_IEP(gi.Pattern(n, a), g.v_cnt, g.e_cnt, 0))
+                for n, a in [(3, "011101110"), (4, "0110100110010110"), (4, "0111101111001100")]]
+        assert gd.batch_counts(jobs) == [gi.pattern_matching(d, s).count for d, s in jobs]
     finally:
         dist.destroy_process_group()
 
