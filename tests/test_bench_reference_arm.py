@@ -23,7 +23,10 @@ def test_reference_arm_prints_its_line(native, oracle):
     assert r.returncode == 0, r.stderr[-2000:]
     line = json.loads(r.stdout.strip().splitlines()[-1])
     assert line["impl"] == "reference" and line["value"] > 0 and line["unit"] == "embeddings/s"
-    assert line["cpu_baseline"]["kind"] == "port" and line["cpu_baseline"]["cores"] >= 1
+    # The reference's own code when its sources were compiled here, else the port.
+    built = os.access(ROOT / "oracle" / "_ref" / "ref_edge_sample", os.X_OK)
+    assert line["cpu_baseline"]["kind"] == ("reference" if built else "port")
+    assert line["cpu_baseline"]["cores"] >= 1
     assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["e2e"]["d2h_bytes_per_step"] == 0
 
 

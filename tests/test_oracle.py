@@ -140,7 +140,7 @@ def test_pivoting_clique_counts_match_enumeration(oracle):
     for g in (gen.erdos_renyi(200, 3000, 1), gen.rmat(9, 8.0, 11), gen.chung_lu(2000, 12000, 2.2, 200.0, 14)):
         piv = oracle.clique_counts_pivot(7, g.vertex, g.edge)
         assert piv[3:7] == [oracle.cliques(k, g.vertex, g.edge) for k in range(3, 7)]
-        for kmax in (3, 5):  # stopping at h = kmax leaves the lower counts as they are
+        for kmax in (3, 5):  # a smaller kmax closes the search earlier; the lower counts stay the same
             assert oracle.clique_counts_pivot(kmax, g.vertex, g.edge) == piv[:kmax + 1]
     k40 = gen.from_edges(40, [(i, j) for i in range(40) for j in range(i + 1, 40)])
     assert oracle.clique_counts_pivot(7, k40.vertex, k40.edge)[1:] == [comb(40, k) for k in range(1, 8)]
@@ -150,3 +150,35 @@ def test_pivoting_clique_counts_match_enumeration(oracle):
     want[0] += 3
     want[1] += 3
     assert oracle.clique_counts_pivot(7, k70.vertex, k70.edge)[1:] == want
+
+
+REF_SAMPLER = Path(__file__).resolve().parents[1] / "oracle" / "_ref" / "ref_edge_sample"
+
+
+@pytest.mark.skipif(not os.access(REF_SAMPLER, os.X_OK), reason="reference sources not compiled here")
+def test_reference_edge_tasks_sum_to_the_oracle_count(oracle, native, tmp_path):
+    """The reference's own per-edge task (oracle/_ref/ref_edge_sample, the CPU
+    baseline's sampler) summed over every directed edge, with the plans the
+    reference makes from the .g header, equals the oracle's whole count, and
+    its redundancy equals this planner's divisor."""
+    import subprocess
+    import graphindor_b200 as gi
+    from graphindor_b200 import gen
+    from conftest import plan_desc
+    pats = [(4, "0111101111001100"), (4, "0110100110010110"), (5, "0101110101010101010011000"),
+            (6, "011100101010110001100011010101001110")]
+    for g in (gen.rmat(10, 12.0, 12), gen.erdos_renyi(500, 4000, 3)):
+        tri = oracle.triangles(g.vertex, g.edge)
+        path = tmp_path / "g.g"
+        gi.write_g(str(path), g.vertex, g.edge, g.max_intersection_size, tri)
+        for iep in (1, 0):
+            # A target far above the sample's time drives the stride down to 1.
+            args = [str(REF_SAMPLER), str(path), str(iep), "1000", "4"] + [x for n, a in pats for x in (str(n), a)]
+            out = subprocess.run(args, capture_output=True, text=True, check=True, timeout=300).stdout
+            rows = {f[0]: f for f in (line.split() for line in out.splitlines() if " raw " in line)}
+            for n, a in pats:
+                f = rows[a]
+                d = plan_desc(gi.Schedule_IEP(gi.Pattern(n, a), g.v_cnt, g.e_cnt, tri, enable_iep=bool(iep)))
+                raw, _ = oracle.count(d, g.vertex, g.edge)
+                assert (int(f[2]), int(f[4]), int(f[6])) == (raw, g.e_cnt, 1), (iep, a)
+                assert int(f[10]) == d.count_divisor, (iep, a)
