@@ -115,3 +115,25 @@ def test_candidates_do_not_depend_on_planning_order(native):
                            text=True, timeout=600)
         assert r.returncode == 0, r.stderr[-2000:]
         assert mine == json.loads(r.stdout), g
+
+
+def test_concurrent_planning_gives_the_sequential_plans(native):
+    """gi_plan_create from eight threads at once (ctypes releases the GIL) in a
+    fresh process, each job twice, so threads race on the same patterns'
+    first plans: every plan equals the one planned alone."""
+    import subprocess
+    import sys
+    from pathlib import Path
+    here = Path(__file__).resolve().parent
+    jobs = [j["job"] for j in JOBS if j["job"].startswith("full")][:160]
+    code = ("import sys, json; sys.path[:0] = [%r, %r]; import test_planner as t\n"
+            "from concurrent.futures import ThreadPoolExecutor\n"
+            "jobs = json.loads(sys.stdin.read())\n"
+            "with ThreadPoolExecutor(max_workers=8) as ex:\n"
+            "    print(json.dumps(list(ex.map(lambda j: t._plan(j).export(), jobs + jobs))))\n"
+            % (str(here), str(here.parent)))
+    r = subprocess.run([sys.executable, "-c", code], input=json.dumps(jobs), capture_output=True, text=True,
+                       timeout=900)
+    assert r.returncode == 0, r.stderr[-2000:]
+    want = [_plan(job).export() for job in jobs]
+    assert json.loads(r.stdout) == want * 2
