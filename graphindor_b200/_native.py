@@ -82,6 +82,7 @@ class LabeledGraphInfo(C.Structure):
 
 GI_FSM_MAX_PATTERNS = 64
 GI_GRAPH_FEATURES = 19
+GI_LEARNED_CANDIDATES = 16  # the analytic model's best valid candidates that the learned model re-ranks
 
 
 class FsmPattern(C.Structure):

@@ -6,6 +6,7 @@
 // fp32) is trained offline on engine-measured times
 // (graphindor_b200/schedule_cost/train.py); the feature layout here must
 // match graphindor_b200/schedule_cost/features.py.
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -173,30 +174,26 @@ int gi_plan_create_learned(int n, const char *adj, int32_t v_cnt, int64_t e_cnt,
         Pattern pat(n, adj);
         if (!pat.check_connected()) return fail(GI_EDISCONNECTED, "pattern is not connected");
         const auto cands = Schedule_IEP::enumerate_candidates(pat, enable_iep != 0, v_cnt, e_cnt, tri_cnt);
-        // Predictions of the valid candidates, in parallel (each one computed
-        // the same way on any thread); the minimum is taken in candidate
-        // order, the first of equal predictions winning.
-        const int64_t nc = static_cast<int64_t>(cands.size());
-        std::vector<float> y(static_cast<size_t>(nc), 0.f);
-#pragma omp parallel
-        {
-            std::vector<float> x(kDim);
-            std::memcpy(x.data() + kPlanDim, graph_features, sizeof(float) * kGraphDim);
-#pragma omp for schedule(dynamic, 16)
-            for (int64_t i = 0; i < nc; ++i) {
-                const auto &c = cands[static_cast<size_t>(i)];
-                if (c.divisor <= 0) continue;
-                plan_features(n, pat.get_adj_mat_ptr(), c.order, c.restricts, c.model_cost, c.iep_k, x.data());
-                y[static_cast<size_t>(i)] = forward(m, x.data());
-            }
-        }
+        // The valid candidates of lowest analytic cost, back in enumeration
+        // order; the first of equal predictions wins.
+        std::vector<int> top;
+        for (size_t i = 0; i < cands.size(); ++i)
+            if (cands[i].divisor > 0) top.push_back(static_cast<int>(i));
+        std::stable_sort(top.begin(), top.end(),
+                         [&](int a, int b) { return cands[a].model_cost < cands[b].model_cost; });
+        if (top.size() > static_cast<size_t>(GI_LEARNED_CANDIDATES)) top.resize(GI_LEARNED_CANDIDATES);
+        std::sort(top.begin(), top.end());
+        std::vector<float> x(kDim);
+        std::memcpy(x.data() + kPlanDim, graph_features, sizeof(float) * kGraphDim);
         int best = -1;
         float best_y = 0.f;
-        for (int64_t i = 0; i < nc; ++i) {
-            if (cands[static_cast<size_t>(i)].divisor <= 0) continue;
-            if (best < 0 || y[static_cast<size_t>(i)] < best_y) {
-                best = static_cast<int>(i);
-                best_y = y[static_cast<size_t>(i)];
+        for (int i : top) {
+            const auto &c = cands[static_cast<size_t>(i)];
+            plan_features(n, pat.get_adj_mat_ptr(), c.order, c.restricts, c.model_cost, c.iep_k, x.data());
+            const float y = forward(m, x.data());
+            if (best < 0 || y < best_y) {
+                best = i;
+                best_y = y;
             }
         }
         if (best < 0) return fail(GI_EINVAL, "pattern has no valid candidate schedule");

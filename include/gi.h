@@ -295,9 +295,13 @@ int gi_cost_model_load(const char *path);
 /* The graph features of a graph handle, or of host CSR offsets. */
 int gi_graph_features(const gi_graph *g, float *out, int cap);
 int gi_graph_features_host(const int64_t *vertex, int32_t v_cnt, int64_t tri_cnt, float *out, int cap);
-/* The valid candidate with the smallest predicted time, as
- * gi_plan_create_explicit builds it (exact counts).  predicted_ms (optional)
- * receives the model's prediction. */
+/* The model re-ranks the GI_LEARNED_CANDIDATES valid candidates of lowest
+ * analytic cost (ties: enumeration order), the region of the candidate space
+ * its training timings cover; the analytic model stays the first filter. */
+#define GI_LEARNED_CANDIDATES 16
+/* Of those, the one with the smallest predicted time (ties: enumeration
+ * order), as gi_plan_create_explicit builds it (exact counts).  predicted_ms
+ * (optional) receives the model's prediction. */
 int gi_plan_create_learned(int n, const char *adj, int32_t v_cnt, int64_t e_cnt, int64_t tri_cnt,
                            const float *graph_features, int enable_iep, gi_plan **out, double *predicted_ms);
 /* Training kernels of that model (3-layer MLP, fp32, ReLU, mean squared

@@ -38,7 +38,10 @@ def test_learned_choice_is_the_python_argmin(tmp_path, native, seed):
     for n, adj in [(5, "0101110101010101010011000"), (6, "011100101010110001100011010101001110"),
                    (4, "0110100110010110")]:
         p = gi.Pattern(n, adj)
-        cands = [c for c in gi.Schedule_IEP.candidates(p, g.v_cnt, g.e_cnt, 777) if c[3] > 0]
+        valid = [c for c in gi.Schedule_IEP.candidates(p, g.v_cnt, g.e_cnt, 777) if c[3] > 0]
+        # The model re-ranks the analytic model's best GI_LEARNED_CANDIDATES, kept in enumeration order.
+        top = sorted(sorted(range(len(valid)), key=lambda i: valid[i][2])[:N.GI_LEARNED_CANDIDATES])
+        cands = [valid[i] for i in top]
         k = gi.Schedule_IEP(p, order=cands[0][0], restricts=cands[0][1]).export()["in_exclusion_optimize_num"]
         X = np.stack([np.concatenate([plan_features(n, adj, o, r, cost, k), gf]) for o, r, cost, _ in cands])
         pred, _ = mlp.forward((X - mu) / sd)
