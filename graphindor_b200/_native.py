@@ -127,6 +127,7 @@ _SIGS = {
                                  C.POINTER(Stats)]),
     "gi_clique_count": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.POINTER(C.c_uint64),
                                   C.POINTER(Stats)]),
+    "gi_clique_counts_pivot": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(Stats)]),
     "gi_motif_num": (C.c_int, [C.c_int]),
     "gi_motif_patterns": (C.c_int, [C.c_int, C.c_char_p, C.c_int]),
     "gi_motif_count": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.POINTER(Stats)]),

@@ -30,6 +30,7 @@ int count_impl(gi_graph *g, const DevPlan &P, cudaStream_t st, uint64_t *raw_sum
                int64_t shard, int64_t num_shards);
 void graph_free(gi_graph *g);
 int kclique_bitmap(gi_graph *o, int k, cudaStream_t st, uint64_t *out, gi_stats *stats);
+int kclique_pivot(gi_graph *o, int kmax, cudaStream_t st, uint64_t *counts, gi_stats *stats);
 int kclique_max_bitmap_degree();
 
 namespace {
@@ -207,6 +208,25 @@ extern "C" int gi_clique_count(const gi_graph *cg, int k, int orientation, gi_st
     if (rc != GI_OK) return rc;
     *out_count = raw;  // redundancy is 1 for the clique plan (reference gpu/gpu_clique.cu:628)
     return GI_OK;
+}
+
+extern "C" int gi_clique_counts_pivot(const gi_graph *cg, int kmax, gi_stream stream, uint64_t *counts,
+                                      gi_stats *stats) {
+    if (!cg || !counts) return fail(GI_EINVAL, "NULL argument");
+    if (kmax < 1 || kmax > GI_MAX_PATTERN) return fail(GI_EINVAL, "kmax must be between 1 and 7");
+    gi_graph *g = const_cast<gi_graph *>(cg);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    std::lock_guard<std::mutex> lock(g->mu);
+    gi_graph *o = nullptr;
+    int rc = oriented_graph(g, 1, st, &o);
+    if (rc != GI_OK) return rc;
+    if (stats) std::memset(stats, 0, sizeof(*stats));
+    if (o->max_degree > kclique_max_bitmap_degree())
+        return fail(GI_ENOTSUP, "an out-degree of the degree-oriented graph exceeds the bitmap limit");
+    std::lock_guard<std::mutex> lock2(o->mu);
+    rc = kclique_pivot(o, kmax, st, counts, stats);
+    if (rc == GI_ENOMEM) return fail(GI_ENOMEM, "k-clique bitmaps do not fit in half the free device memory");
+    return rc;
 }
 
 extern "C" int gi_motif_count(const gi_graph *cg, int k, gi_stream stream, uint64_t *out_counts, int cap,

@@ -28,8 +28,10 @@
 #include <cub/device/device_scan.cuh>
 
 #include <algorithm>
+#include <vector>
 
 #include "internal.hpp"
+#include "pivot.cuh"
 
 namespace gi {
 
@@ -267,6 +269,41 @@ __global__ void __launch_bounds__(kBlock)
     if (lane == 0 && acc) atomicAdd(&counters[kSum], acc);
 }
 
+// Clique-tree pivoting (pivot.cuh): a warp per root vertex, claimed one at a
+// time; counters [0] root cursor, [1] stack overflow, [2 + k] k-cliques.
+__global__ void __launch_bounds__(kBlock)
+    kc_pivot_kernel(const int64_t *__restrict__ vertex, int32_t v_cnt, const int64_t *__restrict__ off,
+                    const uint32_t *__restrict__ bitmap, int kmax, const uint64_t *__restrict__ binom,
+                    pivot::Layout L, uint32_t *scratch, unsigned long long *counters) {
+    const int lane = threadIdx.x & 31;
+    const int64_t warp = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    uint32_t *mine = scratch + warp * L.words();
+    const pivot::WarpLanes wp{lane};
+    uint64_t acc[pivot::kMaxK + 1] = {};
+    bool ok = true;
+    while (true) {
+        unsigned long long v = 0;
+        if (lane == 0) v = atomicAdd(&counters[0], 1ull);
+        v = __shfl_sync(kFull, v, 0);
+        if (v >= static_cast<unsigned long long>(v_cnt)) break;
+        const int d = static_cast<int>(vertex[v + 1] - vertex[v]);
+        if (d > L.dmax) {  // the layout is sized by the largest out-degree
+            ok = false;
+            break;
+        }
+        const uint32_t *D = d >= 2 ? bitmap + off[v] : nullptr;
+        if (!pivot::count_root(wp, D, d, kmax, binom, L, mine, acc)) {
+            ok = false;
+            break;
+        }
+    }
+    if (lane == 0) {
+        if (!ok) atomicExch(&counters[1], 1ull);
+        for (int k = 0; k <= kmax; ++k)
+            if (acc[k]) atomicAdd(&counters[2 + k], static_cast<unsigned long long>(acc[k]));
+    }
+}
+
 }  // namespace
 
 int kclique_max_bitmap_degree() { return 32 * 32 * kWarpWpl; }
@@ -389,4 +426,84 @@ int kclique_bitmap(gi_graph *o, int k, cudaStream_t st, uint64_t *out, gi_stats 
     return GI_OK;
 }
 
+// Counts of every clique size 1..kmax (kmax <= 7) of the degree-oriented DAG
+// `o` at once by clique-tree pivoting: counts[k] = k-cliques (counts[0] = 0).
+// Stack levels start at 64 and grow (up to the largest out-degree + 2) when a
+// search is deeper; the workers' scratch is held to about 1 GiB.
+int kclique_pivot(gi_graph *o, int kmax, cudaStream_t st, uint64_t *counts, gi_stats *stats) {
+    float build_ms = 0.f;
+    int launches = 0;
+    int rc = ensure_bitmaps(o, st, &build_ms, &launches);
+    if (rc != GI_OK) return rc;
+    int sms = 148, per_sm = 1;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, o->device);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kc_pivot_kernel, kBlock, 0);
+    pivot::Layout L;
+    L.dmax = std::max<int64_t>(o->max_degree, 1);
+    L.wmax = std::max<int64_t>((L.dmax + 31) / 32, 1);
+    const int64_t max_levels = L.dmax + 2;
+    L.levels = std::min<int64_t>(64, max_levels);
+    float total_ms = 0.f;
+    while (true) {
+        const size_t per_warp = static_cast<size_t>(L.words()) * sizeof(uint32_t);
+        const int64_t fit = std::max<int64_t>(1, (int64_t(1) << 30) / static_cast<int64_t>(per_warp) / kWarps);
+        const int blocks = static_cast<int>(std::min<int64_t>(static_cast<int64_t>(sms) * std::max(per_sm, 1), fit));
+        uint32_t *scratch = nullptr;
+        uint64_t *binom = nullptr;
+        unsigned long long *ctr = nullptr;
+        cudaError_t e = cudaMalloc(&scratch, per_warp * static_cast<size_t>(blocks) * kWarps);
+        const int64_t rows = L.levels + 1;
+        std::vector<uint64_t> hb(static_cast<size_t>(rows) * pivot::kBinomCols, 0);
+        for (int64_t q = 0; q < rows; ++q)
+            for (int j = 0; j < pivot::kBinomCols; ++j)
+                hb[q * pivot::kBinomCols + j] =
+                    j == 0 ? 1 : (q == 0 ? 0 : hb[(q - 1) * pivot::kBinomCols + j - 1] + hb[(q - 1) * pivot::kBinomCols + j]);
+        if (e == cudaSuccess) e = cudaMalloc(&binom, hb.size() * sizeof(uint64_t));
+        if (e == cudaSuccess) e = cudaMalloc(&ctr, 16 * sizeof(unsigned long long));
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(binom, hb.data(), hb.size() * sizeof(uint64_t), cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess) e = cudaMemsetAsync(ctr, 0, 16 * sizeof(unsigned long long), st);
+        cudaEvent_t t0 = nullptr, t1 = nullptr;
+        unsigned long long host[16] = {0};
+        float ms = 0.f;
+        if (e == cudaSuccess) {
+            cudaEventCreate(&t0);
+            cudaEventCreate(&t1);
+            cudaEventRecord(t0, st);
+            kc_pivot_kernel<<<blocks, kBlock, 0, st>>>(o->d_vertex, o->v_cnt, o->d_bitmap_off, o->d_bitmap, kmax,
+                                                       binom, L, scratch, ctr);
+            e = cudaGetLastError();
+            cudaEventRecord(t1, st);
+            if (e == cudaSuccess) e = cudaMemcpyAsync(host, ctr, sizeof(host), cudaMemcpyDeviceToHost, st);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+            if (e == cudaSuccess) cudaEventElapsedTime(&ms, t0, t1);
+            cudaEventDestroy(t0);
+            cudaEventDestroy(t1);
+        }
+        cudaFree(scratch);
+        cudaFree(binom);
+        cudaFree(ctr);
+        if (e != cudaSuccess) return cuda_fail(e, "clique-tree pivoting kernel");
+        ++launches;
+        total_ms += ms;
+        if (host[1] == 0) {
+            counts[0] = 0;
+            for (int k = 1; k <= kmax; ++k) counts[k] = host[2 + k];
+            if (stats) {
+                stats->kernel_ms = total_ms + build_ms;
+                stats->prep_ms = build_ms;
+                stats->raw_sum = counts[kmax];
+                stats->tasks = static_cast<uint64_t>(o->v_cnt);
+                stats->kernel_launches = launches;
+                stats->grid_blocks = blocks;
+                stats->block_threads = kBlock;
+            }
+            return GI_OK;
+        }
+        if (L.levels >= max_levels) return fail(GI_EOVERFLOW, "clique-tree pivoting: search deeper than its stack");
+        L.levels = std::min<int64_t>(L.levels * 4, max_levels);
+    }
+}
+
 }  // namespace gi
+

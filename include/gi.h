@@ -257,6 +257,16 @@ int gi_count_noalloc(const int64_t *d_vertex, const int32_t *d_edge, int32_t v_c
 int gi_clique_count(const gi_graph *g, int k, int orientation, gi_stream stream, uint64_t *out_count,
                     gi_stats *stats);
 
+/* No reference counterpart (the reference enumerates, gpu/gpu_kclique.cu).
+ * The number of k-cliques for every k in [1, kmax] at once, counts[k]
+ * (counts needs kmax + 1 entries; counts[0] = 0), by clique-tree pivoting
+ * (Jain and Seshadhri, WSDM 2020) on the degree-oriented DAG's per-vertex
+ * bitmaps, which gi_clique_count(..., 1) builds and keeps: one warp per root
+ * vertex, cost growing with the pivot tree rather than with the number of
+ * cliques.  1 <= kmax <= 7.  GI_ENOTSUP when an out-degree exceeds the
+ * bitmap limit (4096), GI_ENOMEM when the bitmaps do not fit. */
+int gi_clique_counts_pivot(const gi_graph *g, int kmax, gi_stream stream, uint64_t *counts, gi_stats *stats);
+
 /* Replaces gpu_mc (reference gpu/gpu_mc.cu:62-119): edge-induced counts of
  * every connected k-vertex pattern in the reference MotifGenerator order
  * (reference src/motif_generator.cpp:5-43).  out_counts needs room for
