@@ -432,7 +432,9 @@ def run_batch(args):
     """Batched serving: 64 seeded random connected patterns of 4-6 vertices
     (edge density 0.4-1.0) against 8 seeded R-MAT graphs of scales 10-12
     (edge factor 8-16), all 512 jobs in one persistent launch replayed from a
-    CUDA graph, against one gi_count launch per job; counts must agree."""
+    CUDA graph, against one gi_count launch per job; counts must agree.  Also
+    end to end with planning: learned plans in one batch against analytic
+    plans with one launch per job."""
     import random
 
     import torch
@@ -444,12 +446,31 @@ def run_batch(args):
     graphs = []
     for i in range(8):
         g = gen.rmat(rng.randint(10, 12), rng.uniform(8, 16), 100 + i)
-        graphs.append(gi.Graph.from_csr(g.vertex, g.edge))
+        dg = gi.Graph.from_csr(g.vertex, g.edge)
+        tri = gi.clique_count(dg, 3, 1).count  # the triangle count the analytic model plans with
+        graphs.append(gi.Graph.from_csr(g.vertex, g.edge, tri_cnt=tri))
     pats = []
     for _ in range(64):
         n = rng.randint(4, 6)
         pats.append((n, random_connected(n, rng.uniform(0.4, 1.0), rng)))
-    jobs = [(g, gi.Schedule_IEP(gi.Pattern(n, adj), g.v_cnt, g.e_cnt, 0)) for g in graphs for n, adj in pats]
+    # End to end first, while no plan of these patterns is kept yet: the
+    # engine's path (learned selection, one batched launch from a CUDA graph)
+    # against the reference's way (analytic plans, one launch per job), each
+    # planning every job; graphs are resident for both.
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    ljobs = [(g, gi.Schedule_IEP.learned(gi.Pattern(n, adj), g)) for g in graphs for n, adj in pats]
+    lcounts, _, _ = gi.Batch(ljobs).run()
+    e2e_learned_batched = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    jobs, pcounts = [], []
+    for g in graphs:
+        for n, adj in pats:
+            s = gi.Schedule_IEP(gi.Pattern(n, adj), g.v_cnt, g.e_cnt, g.tri_cnt)
+            jobs.append((g, s))
+            pcounts.append(gi.pattern_matching(g, s).count)
+    e2e_analytic_single = time.perf_counter() - t0
+    assert lcounts == pcounts
     batch = gi.Batch(jobs)
     for _ in range(max(1, args.warmup)):
         counts, _, _ = batch.run()
@@ -488,7 +509,10 @@ def run_batch(args):
                        "one_launch_per_job": {"jobs_per_s_device": len(jobs) / (sum(single) / 1e3),
                                               "jobs_per_s_wall": len(jobs) / t_all,
                                               "job_ms_p50": pct(sorted(single), 0.5),
-                                              "job_ms_p99": pct(sorted(single), 0.99)}}}
+                                              "job_ms_p99": pct(sorted(single), 0.99)},
+                       "end_to_end_s": {"learned_plans_one_batch": e2e_learned_batched,
+                                        "analytic_plans_one_launch_per_job": e2e_analytic_single,
+                                        "speedup": e2e_analytic_single / max(e2e_learned_batched, 1e-9)}}}
 
 
 def main():

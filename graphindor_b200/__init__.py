@@ -131,9 +131,10 @@ class Schedule_IEP:
     @classmethod
     def learned(cls, pattern: Pattern, graph: "Graph", enable_iep: bool = True,
                 model_path: Optional[str] = None) -> "Schedule_IEP":
-        """The valid candidate schedule with the smallest device time the
-        learned cost model predicts on `graph` (exact counts).  Loads the
-        package's trained model on first use unless model_path is given."""
+        """Of the analytic model's GI_LEARNED_CANDIDATES best valid candidate
+        schedules, the one with the smallest device time the learned cost
+        model predicts on `graph` (exact counts).  Loads the package's trained
+        model on first use unless model_path is given."""
         L = lib()
         load_cost_model(model_path)
         feats = (C.c_float * N.GI_GRAPH_FEATURES)()
