@@ -1,8 +1,8 @@
-// Learned schedule cost model: ranks the valid candidate schedules of a
-// pattern (vertex order + restriction set, reference
-// src/schedule_IEP.cpp:67-189 enumerates them) by the device time a small
-// MLP predicts for them on a graph, instead of the reference's analytic
-// model (src/schedule_IEP.cpp:307-382).  The MLP (3 layers, hidden 128,
+// Learned schedule cost model: re-ranks the analytic model's best valid
+// candidate schedules of a pattern (vertex order + restriction set,
+// reference src/schedule_IEP.cpp:67-189 enumerates them; the analytic model
+// is src/schedule_IEP.cpp:307-382) by the device time a small MLP predicts
+// for them on a graph.  The MLP (3 layers, hidden 128,
 // fp32) is trained offline on engine-measured times
 // (graphindor_b200/schedule_cost/train.py); the feature layout here must
 // match graphindor_b200/schedule_cost/features.py.

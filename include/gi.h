@@ -295,9 +295,9 @@ int gi_batch_destroy(gi_batch *b);
 
 /* No reference counterpart: the reference picks a schedule with its analytic
  * model only (src/schedule_IEP.cpp:307-382).  A small MLP trained on
- * engine-measured device times (graphindor_b200/schedule_cost/train.py) ranks
- * the valid candidate schedules (order + restriction set) of a pattern for a
- * graph described by GI_GRAPH_FEATURES floats. */
+ * engine-measured device times (graphindor_b200/schedule_cost/train.py)
+ * re-ranks the best valid candidate schedules (order + restriction set) of a
+ * pattern for a graph described by GI_GRAPH_FEATURES floats. */
 #define GI_GRAPH_FEATURES 19
 /* Loads the model file written by train.py (process-wide; replaces any
  * loaded model). */
