@@ -270,11 +270,14 @@ __global__ void __launch_bounds__(kBlock)
 }
 
 // Clique-tree pivoting (pivot.cuh): a warp per root vertex, claimed one at a
-// time; counters [0] root cursor, [1] stack overflow, [2 + k] k-cliques.
+// time in the order of `roots` (largest out-degree first, so that the
+// heaviest searches start early); counters [0] root cursor, [1] stack
+// overflow, [2 + k] k-cliques.
 __global__ void __launch_bounds__(kBlock)
-    kc_pivot_kernel(const int64_t *__restrict__ vertex, int32_t v_cnt, const int64_t *__restrict__ off,
-                    const uint32_t *__restrict__ bitmap, int kmax, const uint64_t *__restrict__ binom,
-                    pivot::Layout L, uint32_t *scratch, unsigned long long *counters) {
+    kc_pivot_kernel(const int64_t *__restrict__ vertex, int32_t v_cnt, const int32_t *__restrict__ roots,
+                    const int64_t *__restrict__ off, const uint32_t *__restrict__ bitmap, int kmax,
+                    const uint64_t *__restrict__ binom, pivot::Layout L, uint32_t *scratch,
+                    unsigned long long *counters) {
     const int lane = threadIdx.x & 31;
     const int64_t warp = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
     uint32_t *mine = scratch + warp * L.words();
@@ -282,10 +285,11 @@ __global__ void __launch_bounds__(kBlock)
     uint64_t acc[pivot::kMaxK + 1] = {};
     bool ok = true;
     while (true) {
-        unsigned long long v = 0;
-        if (lane == 0) v = atomicAdd(&counters[0], 1ull);
-        v = __shfl_sync(kFull, v, 0);
-        if (v >= static_cast<unsigned long long>(v_cnt)) break;
+        unsigned long long c = 0;
+        if (lane == 0) c = atomicAdd(&counters[0], 1ull);
+        c = __shfl_sync(kFull, c, 0);
+        if (c >= static_cast<unsigned long long>(v_cnt)) break;
+        const int64_t v = roots[c];
         const int d = static_cast<int>(vertex[v + 1] - vertex[v]);
         if (d > L.dmax) {  // the layout is sized by the largest out-degree
             ok = false;
@@ -443,6 +447,33 @@ int kclique_pivot(gi_graph *o, int kmax, cudaStream_t st, uint64_t *counts, gi_s
     L.wmax = std::max<int64_t>((L.dmax + 31) / 32, 1);
     const int64_t max_levels = L.dmax + 2;
     L.levels = std::min<int64_t>(64, max_levels);
+    // Roots by out-degree, largest first (counting sort on the host; ties in
+    // id order).
+    int32_t *d_roots = nullptr;
+    {
+        std::vector<int64_t> hv(static_cast<size_t>(o->v_cnt) + 1);
+        cudaError_t e = cudaMemcpyAsync(hv.data(), o->d_vertex, hv.size() * sizeof(int64_t), cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) return cuda_fail(e, "out-degrees for the root order");
+        // Bucket of v: L.dmax - out-degree, clamped into [0, L.dmax].
+        auto bucket = [&](int32_t v) {
+            const int64_t d = hv[v + 1] - hv[v];
+            return static_cast<size_t>(L.dmax - std::min<int64_t>(std::max<int64_t>(d, 0), L.dmax));
+        };
+        std::vector<int64_t> start(static_cast<size_t>(L.dmax) + 2, 0);
+        for (int32_t v = 0; v < o->v_cnt; ++v) ++start[bucket(v) + 1];
+        for (size_t i = 1; i < start.size(); ++i) start[i] += start[i - 1];
+        std::vector<int32_t> order(static_cast<size_t>(o->v_cnt));
+        for (int32_t v = 0; v < o->v_cnt; ++v) order[static_cast<size_t>(start[bucket(v)]++)] = v;
+        if ((e = cudaMalloc(&d_roots, order.size() * sizeof(int32_t) + sizeof(int32_t))) != cudaSuccess)
+            return cuda_fail(e, "root order");
+        if ((e = cudaMemcpyAsync(d_roots, order.data(), order.size() * sizeof(int32_t), cudaMemcpyHostToDevice, st)) !=
+                cudaSuccess ||
+            (e = cudaStreamSynchronize(st)) != cudaSuccess) {
+            cudaFree(d_roots);
+            return cuda_fail(e, "root order");
+        }
+    }
     float total_ms = 0.f;
     while (true) {
         const size_t per_warp = static_cast<size_t>(L.words()) * sizeof(uint32_t);
@@ -470,8 +501,8 @@ int kclique_pivot(gi_graph *o, int kmax, cudaStream_t st, uint64_t *counts, gi_s
             cudaEventCreate(&t0);
             cudaEventCreate(&t1);
             cudaEventRecord(t0, st);
-            kc_pivot_kernel<<<blocks, kBlock, 0, st>>>(o->d_vertex, o->v_cnt, o->d_bitmap_off, o->d_bitmap, kmax,
-                                                       binom, L, scratch, ctr);
+            kc_pivot_kernel<<<blocks, kBlock, 0, st>>>(o->d_vertex, o->v_cnt, d_roots, o->d_bitmap_off,
+                                                       o->d_bitmap, kmax, binom, L, scratch, ctr);
             e = cudaGetLastError();
             cudaEventRecord(t1, st);
             if (e == cudaSuccess) e = cudaMemcpyAsync(host, ctr, sizeof(host), cudaMemcpyDeviceToHost, st);
@@ -483,10 +514,14 @@ int kclique_pivot(gi_graph *o, int kmax, cudaStream_t st, uint64_t *counts, gi_s
         cudaFree(scratch);
         cudaFree(binom);
         cudaFree(ctr);
-        if (e != cudaSuccess) return cuda_fail(e, "clique-tree pivoting kernel");
+        if (e != cudaSuccess) {
+            cudaFree(d_roots);
+            return cuda_fail(e, "clique-tree pivoting kernel");
+        }
         ++launches;
         total_ms += ms;
         if (host[1] == 0) {
+            cudaFree(d_roots);
             counts[0] = 0;
             for (int k = 1; k <= kmax; ++k) counts[k] = host[2 + k];
             if (stats) {
@@ -500,7 +535,10 @@ int kclique_pivot(gi_graph *o, int kmax, cudaStream_t st, uint64_t *counts, gi_s
             }
             return GI_OK;
         }
-        if (L.levels >= max_levels) return fail(GI_EOVERFLOW, "clique-tree pivoting: search deeper than its stack");
+        if (L.levels >= max_levels) {
+            cudaFree(d_roots);
+            return fail(GI_EOVERFLOW, "clique-tree pivoting: search deeper than its stack");
+        }
         L.levels = std::min<int64_t>(L.levels * 4, max_levels);
     }
 }
