@@ -268,6 +268,21 @@ def pattern_matching(graph: Graph, schedule: Schedule_IEP, *, count_bytes: bool 
     return _result(out.value, s)
 
 
+def count_edges(graph: Graph, schedule: Schedule_IEP, edge_step: int, edge_offset: int = 0, *, shard: int = 0,
+                num_shards: int = 1, count_bytes: bool = False, stream: int = 0) -> N.Stats:
+    """Raw sum (modulo 2^64, not divided) of the first-level tasks of the
+    directed edges e with e % edge_step == edge_offset (gi_count_shard's edge
+    subset): the reference's per-edge task summed over exactly those edges.
+    Returns the gi_stats of the call (raw_sum, kernel_ms, chunks, ...)."""
+    s = _stats(count_bytes)
+    s.edge_step = int(edge_step)
+    s.edge_offset = int(edge_offset)
+    raw = C.c_uint64()
+    check(lib().gi_count_shard(graph.handle, schedule.handle, int(shard), int(num_shards),
+                               C.c_void_p(stream) if stream else None, C.byref(raw), C.byref(s)), "gi_count_shard")
+    return s
+
+
 def clique_count(graph: Graph, k: int, orientation: int = 0, *, count_bytes: bool = False,
                  stream: int = 0) -> CountResult:
     out = C.c_uint64()

@@ -73,7 +73,8 @@ class Stats(C.Structure):
                 ("alg_bytes", C.c_uint64), ("count_bytes", C.c_int32), ("budget_ms", C.c_double),
                 ("grid_blocks", C.c_int32), ("block_threads", C.c_int32), ("kernel_launches", C.c_int32),
                 ("allow_partial", C.c_int32), ("chunks_done", C.c_int64), ("chunks_total", C.c_int64),
-                ("prep_ms", C.c_double), ("sample_chunks", C.c_int64)]
+                ("prep_ms", C.c_double), ("sample_chunks", C.c_int64), ("edge_step", C.c_int64),
+                ("edge_offset", C.c_int64)]
 
 
 class LabeledGraphInfo(C.Structure):

@@ -45,13 +45,16 @@ namespace {
 
 // Subtasks per edge: a degree bound on the depth-2 loop set, cut into
 // pieces of `split` candidates; 0 for edges the depth-1 restriction drops.
+// With edge_step > 1 only the edges i with i % edge_step == edge_offset get
+// subtasks (an edge subset).
 __global__ void split_count_kernel(const __grid_constant__ DevPlan P, const int64_t *__restrict__ vertex,
                                    const uint32_t *__restrict__ edge, const uint32_t *__restrict__ edge_from,
-                                   int64_t e_cnt, int split, int64_t *__restrict__ counts) {
+                                   int64_t e_cnt, int split, int64_t edge_step, int64_t edge_offset,
+                                   int64_t *__restrict__ counts) {
     const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
     for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < e_cnt; i += stride) {
         const uint32_t v0 = edge_from[i], v1 = edge[i];
-        if (P.first_restricted && v0 <= v1) {
+        if ((P.first_restricted && v0 <= v1) || (edge_step > 1 && i % edge_step != edge_offset)) {
             counts[i] = 0;
             continue;
         }
@@ -79,7 +82,8 @@ __global__ void __launch_bounds__(kBlockThreads, kMinBlocks)
                      int64_t slot_stride, unsigned long long *counters, unsigned long long budget_ns, int64_t shard,
                      int64_t num_shards, int64_t n_chunks, int64_t perm_a, int64_t perm_b,
                      unsigned long long hard_ns, unsigned long long max_claims, Handoff *hitems,
-                     unsigned long long hcap, uint32_t hepoch, uint32_t v_cnt) {
+                     unsigned long long hcap, uint32_t hepoch, uint32_t v_cnt, int64_t edge_step,
+                     int64_t edge_offset) {
     __shared__ WarpState states[kWarpsPerBlock];
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
@@ -127,7 +131,7 @@ __global__ void __launch_bounds__(kBlockThreads, kMinBlocks)
         const int64_t base = chunk * kTaskChunk;
         const int64_t t = base + lane;
         bool valid = t < n_tasks;
-        int64_t e = t;
+        int64_t e = edge_offset + t * edge_step;  // without the split, work item t is the t-th edge of the subset
         int lo = 0;
         if (valid && offsets) {
             // Edge of subtask t: the last e with offsets[e] <= t.
@@ -286,7 +290,8 @@ static int split_size(const DevPlan &P) { return P.leaf_depth == 2 ? GI_SPLIT_LE
 
 // Builds the subtask offsets for the plan's depth-2 split; returns the
 // number of subtasks.  Caller holds g->mu.
-static int build_split(gi_graph *g, const DevPlan &P, cudaStream_t st, int split, int64_t *n_tasks) {
+static int build_split(gi_graph *g, const DevPlan &P, cudaStream_t st, int split, int64_t edge_step,
+                       int64_t edge_offset, int64_t *n_tasks) {
     cudaError_t e;
     const size_t n = static_cast<size_t>(g->e_cnt) + 1;
     if (!g->d_offsets) {
@@ -308,7 +313,8 @@ static int build_split(gi_graph *g, const DevPlan &P, cudaStream_t st, int split
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, g->device);
     if ((e = cudaMemsetAsync(counts + g->e_cnt, 0, sizeof(int64_t), st)) != cudaSuccess) return cuda_fail(e, "memset");
     split_count_kernel<<<sms * 16, 256, 0, st>>>(P, g->d_vertex, reinterpret_cast<const uint32_t *>(g->d_edge),
-                                                  g->d_edge_from, g->e_cnt, split, counts);
+                                                  g->d_edge_from, g->e_cnt, split, edge_step, edge_offset,
+                                                  counts);
     if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "split count kernel");
     size_t tmp = g->scan_tmp_bytes;
     if ((e = cub::DeviceScan::ExclusiveSum(g->d_scan_tmp, tmp, counts, g->d_offsets, static_cast<int64_t>(n), st)) !=
@@ -337,12 +343,14 @@ DfsKernel pick_dfs_kernel(bool bytes_on, int n) {
 // budget_ms = 0 means no budget.
 int count_impl(gi_graph *g, const DevPlan &P, cudaStream_t st, uint64_t *raw_sum, gi_stats *stats,
                double budget_ms, int64_t shard, int64_t num_shards) {
-    int prev = 0;
-    cudaGetDevice(&prev);
-    if (prev != g->device) cudaSetDevice(g->device);
+    DeviceGuard device(g->device);
     int sms = 148, blocks_per_sm = 1;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, g->device);
     const bool bytes_on = stats && stats->count_bytes;
+    // Edge subset: the directed edges e with e % edge_step == edge_offset.
+    const int64_t edge_step = stats && stats->edge_step > 1 ? stats->edge_step : 1;
+    const int64_t edge_offset = edge_step > 1 ? stats->edge_offset : 0;
+    if (edge_offset < 0 || edge_offset >= edge_step) return fail(GI_EINVAL, "edge_offset outside [0, edge_step)");
     cudaError_t e;
     const auto kernel = pick_dfs_kernel(bytes_on, P.n);
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, kernel, kBlockThreads, 0);
@@ -353,25 +361,20 @@ int count_impl(gi_graph *g, const DevPlan &P, cudaStream_t st, uint64_t *raw_sum
     const size_t need = static_cast<size_t>(warps) * std::max(P.n_slots, 1) * stride * sizeof(uint32_t);
     int st_code = ensure_scratch(g, need);
     if (st_code != GI_OK) return st_code;
-    cudaEvent_t t0, tm, t1;
-    cudaEventCreate(&t0);
-    cudaEventCreate(&tm);
-    cudaEventCreate(&t1);
+    ScopedEvents ev(3);
+    cudaEvent_t t0 = static_cast<cudaEvent_t>(ev[0]), tm = static_cast<cudaEvent_t>(ev[1]),
+                t1 = static_cast<cudaEvent_t>(ev[2]);
+    if (!t0 || !tm || !t1) return fail(GI_ECUDA, "timing event creation failed");
     cudaEventRecord(t0, st);
     // Split the depth-2 loop when the plan has one; otherwise a work item is
-    // an edge.
+    // an edge of the subset.
     const bool use_split = P.loop2_kind >= 0 && g->e_cnt > 0;
     const int split = split_size(P);
-    int64_t n_tasks = g->e_cnt;
+    int64_t n_tasks = g->e_cnt > edge_offset ? (g->e_cnt - edge_offset + edge_step - 1) / edge_step : 0;
     int launches = 0;
     if (use_split) {
-        st_code = build_split(g, P, st, split, &n_tasks);
-        if (st_code != GI_OK) {
-            cudaEventDestroy(t0);
-            cudaEventDestroy(tm);
-            cudaEventDestroy(t1);
-            return st_code;
-        }
+        st_code = build_split(g, P, st, split, edge_step, edge_offset, &n_tasks);
+        if (st_code != GI_OK) return st_code;
         launches += 1;  // split count (the scan is cub's)
     }
     if ((e = cudaMemsetAsync(g->d_counters, 0, kCounterSlots * sizeof(unsigned long long), st)) != cudaSuccess)
@@ -426,22 +429,17 @@ int count_impl(gi_graph *g, const DevPlan &P, cudaStream_t st, uint64_t *raw_sum
                                              static_cast<uint32_t *>(g->d_scratch), stride, g->d_counters, budget_ns,
                                              shard, num_shards, n_chunks, perm_a, perm_b, hard_ns, max_claims,
                                              hitems, kHandoffCap, g->handoff_epoch,
-                                             static_cast<uint32_t>(g->v_cnt));
+                                             static_cast<uint32_t>(g->v_cnt), edge_step, edge_offset);
     launches += 1;
     e = cudaGetLastError();
     cudaEventRecord(t1, st);
     unsigned long long host[kCounterSlots] = {0};
     if (e == cudaSuccess) e = cudaMemcpyAsync(host, g->d_counters, sizeof(host), cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-    float ms = 0.f, prep = 0.f;
-    if (e == cudaSuccess) {
-        cudaEventElapsedTime(&prep, t0, tm);
-        cudaEventElapsedTime(&ms, tm, t1);
-    }
-    cudaEventDestroy(t0);
-    cudaEventDestroy(tm);
-    cudaEventDestroy(t1);
     if (e != cudaSuccess) return cuda_fail(e, "counting kernel");
+    float ms = 0.f, prep = 0.f;
+    cudaEventElapsedTime(&prep, t0, tm);
+    cudaEventElapsedTime(&ms, tm, t1);
     if (host[kLost]) return fail(GI_ECUDA, "a handed-off work item was never published");
     if (host[kTimeout] && !partial) return fail(GI_ETIMEOUT, "count exceeded its device time budget");
     *raw_sum = host[kSum];
@@ -457,7 +455,6 @@ int count_impl(gi_graph *g, const DevPlan &P, cudaStream_t st, uint64_t *raw_sum
         stats->block_threads = kBlockThreads;
         stats->kernel_launches += launches;
     }
-    if (prev != g->device) cudaSetDevice(prev);
     return GI_OK;
 }
 
@@ -471,8 +468,11 @@ static void reset_stats(gi_stats *stats, double &budget) {
     const int cb = stats->count_bytes;
     const int partial = stats->allow_partial;
     const int64_t sample = stats->sample_chunks;
+    const int64_t step = stats->edge_step, offset = stats->edge_offset;
     budget = stats->budget_ms;
     std::memset(stats, 0, sizeof(*stats));
+    stats->edge_step = step;
+    stats->edge_offset = offset;
     stats->count_bytes = cb;
     stats->budget_ms = budget;
     stats->allow_partial = partial;
@@ -490,6 +490,8 @@ extern "C" int gi_count(const gi_graph *cg, const gi_plan *p, gi_stream stream, 
     if (stats) {  // samples are a gi_count_shard feature; a whole count is whole
         stats->allow_partial = 0;
         stats->sample_chunks = 0;
+        stats->edge_step = 0;
+        stats->edge_offset = 0;
     }
     const int st = count_impl(g, p->dev, static_cast<cudaStream_t>(stream), &raw, stats, budget, 0, 1);
     if (st != GI_OK) return st;

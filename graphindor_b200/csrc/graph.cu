@@ -66,6 +66,31 @@ int cuda_fail(cudaError_t e, const char *what) {
     return fail(e == cudaErrorMemoryAllocation ? GI_ENOMEM : GI_ECUDA, buf);
 }
 
+DeviceGuard::DeviceGuard(int device) : device_(device) {
+    cudaGetDevice(&prev_);
+    if (prev_ != device_) cudaSetDevice(device_);
+}
+
+DeviceGuard::~DeviceGuard() {
+    if (prev_ >= 0 && prev_ != device_) cudaSetDevice(prev_);
+}
+
+ScopedEvents::ScopedEvents(int n) : n_(n < 4 ? n : 4) {
+    for (int i = 0; i < n_; ++i) {
+        cudaEvent_t e = nullptr;
+        if (cudaEventCreate(&e) != cudaSuccess) {
+            cudaGetLastError();
+            e = nullptr;
+        }
+        ev_[i] = e;
+    }
+}
+
+ScopedEvents::~ScopedEvents() {
+    for (int i = 0; i < n_; ++i)
+        if (ev_[i]) cudaEventDestroy(static_cast<cudaEvent_t>(ev_[i]));
+}
+
 void graph_free(gi_graph *g) {
     if (!g) return;
     for (auto *o : g->oriented) graph_free(o);
@@ -82,6 +107,7 @@ void graph_free(gi_graph *g) {
     cudaFree(g->d_handoff);
     cudaFree(g->d_bitmap);
     cudaFree(g->d_bitmap_off);
+    cudaFree(g->d_roots);
     cudaSetDevice(prev);
     delete g;
 }

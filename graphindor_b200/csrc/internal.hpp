@@ -21,6 +21,33 @@ int fail(int status, const std::string &msg);
 // the full list).
 std::vector<std::vector<int>> motif_list(int k, int max_edges = 1 << 30);
 
+// Makes `device` current for a scope and restores the caller's device on
+// every exit path.
+class DeviceGuard {
+  public:
+    explicit DeviceGuard(int device);
+    ~DeviceGuard();
+    DeviceGuard(const DeviceGuard &) = delete;
+    DeviceGuard &operator=(const DeviceGuard &) = delete;
+
+  private:
+    int prev_ = -1, device_ = -1;
+};
+
+// CUDA events (timing) destroyed with the scope.
+class ScopedEvents {
+  public:
+    explicit ScopedEvents(int n);
+    ~ScopedEvents();
+    ScopedEvents(const ScopedEvents &) = delete;
+    ScopedEvents &operator=(const ScopedEvents &) = delete;
+    void *operator[](int i) const { return ev_[i]; }  // a cudaEvent_t
+
+  private:
+    void *ev_[4] = {nullptr, nullptr, nullptr, nullptr};
+    int n_ = 0;
+};
+
 // Per-prefix build mode used by the counting kernels.
 enum PrefixMode : int32_t {
     kAlias = 0,        // father == -1: the set is N(v) itself, no copy
@@ -110,4 +137,7 @@ struct gi_graph {
     uint32_t *d_bitmap = nullptr;
     int64_t *d_bitmap_off = nullptr;  // v_cnt + 1 word offsets
     int64_t bitmap_words = 0;
+    // Roots of the clique-tree pivoting search, largest out-degree first
+    // (kclique.cu), built with the bitmaps' first pivoting count and kept.
+    int32_t *d_roots = nullptr;
 };

@@ -203,6 +203,12 @@ typedef struct gi_stats {
                                 sample_chunks chunks of the shard in the same fixed pseudo-random
                                 order, all of them to completion: a uniform sample whose chunks,
                                 and hence raw_sum, are the same on every call */
+    int64_t edge_step;       /* in (gi_count_shard only): > 1 = count only the first-level tasks of
+                                the directed edges e with e % edge_step == edge_offset, each whole:
+                                the raw sum the reference's per-edge task (reference
+                                src/graph.cpp:392-427) gives summed over exactly those edges.
+                                Subsets of offsets 0 .. edge_step-1 add up to the whole count */
+    int64_t edge_offset;     /* in: 0 <= edge_offset < edge_step */
 } gi_stats;
 
 /* Replaces gpu_pattern_matching<<<...>>> + the D2H of dev_sum + the

@@ -305,10 +305,13 @@ static void edge_task(dfs_t *s, int32_t v0, int32_t v1) {
 }
 
 int oracle_count_edges_timed(const gi_plan_desc *P, const int64_t *vertex, const int32_t *edge, int32_t v_cnt,
-                             int64_t stride, int threads, double max_seconds, uint64_t *raw_sum, int64_t *processed) {
-    if (!P || !vertex || !raw_sum || P->size < 3 || P->size > GI_MAX_PATTERN || v_cnt < 1 || stride < 1) return -1;
+                             int64_t stride, int64_t offset, int threads, double max_seconds, uint64_t *raw_sum,
+                             int64_t *processed) {
+    if (!P || !vertex || !raw_sum || P->size < 3 || P->size > GI_MAX_PATTERN || v_cnt < 1 || stride < 1 ||
+        offset < 0 || offset >= stride)
+        return -1;
     const int64_t e_cnt = vertex[v_cnt];
-    const int64_t n_edges = (e_cnt + stride - 1) / stride;
+    const int64_t n_edges = offset < e_cnt ? (e_cnt - offset + stride - 1) / stride : 0;
     const double deadline = max_seconds > 0 ? omp_get_wtime() + max_seconds : 0.0;
     int max_deg = 1;
     for (int32_t v = 0; v < v_cnt; ++v) {
@@ -333,7 +336,7 @@ int oracle_count_edges_timed(const gi_plan_desc *P, const int64_t *vertex, const
 #pragma omp for schedule(dynamic, 64) nowait
         for (int64_t it = 0; it < n_edges; ++it) {
             if (deadline > 0 && omp_get_wtime() > deadline) continue;
-            const int64_t e = it * stride;
+            const int64_t e = offset + it * stride;
             /* source vertex: the last v with vertex[v] <= e */
             int32_t lo = 0, hi = v_cnt;
             while (hi - lo > 1) {

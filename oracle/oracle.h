@@ -46,14 +46,16 @@ int oracle_count_strided(const gi_plan_desc *plan, const int64_t *vertex, const 
 int oracle_count_timed(const gi_plan_desc *plan, const int64_t *vertex, const int32_t *edge, int32_t v_cnt,
                        int32_t stride, int threads, double max_seconds, uint64_t *raw_sum, int64_t *processed);
 
-/* The same count over the directed edges e = 0, stride, 2*stride, ...: the
- * reference's depth-1 loop entered per sampled edge (summed over all edges
- * it is the whole count).  No edge is begun once max_seconds have passed
- * (0 = no limit); *processed receives how many were counted.  The sampling
- * unit of the timed CPU baseline: finer than a start vertex, whose work a
- * single hub can dominate. */
+/* The same count over the directed edges e = offset, offset + stride,
+ * offset + 2*stride, ... (0 <= offset < stride): the reference's depth-1
+ * loop entered per sampled edge (reference src/graph.cpp:392-427; summed
+ * over all offsets it is the whole count).  No edge is begun once
+ * max_seconds have passed (0 = no limit); *processed receives how many were
+ * counted.  The sampling unit of the timed CPU baseline and the edge subset
+ * of the engine's gi_stats.edge_step / edge_offset. */
 int oracle_count_edges_timed(const gi_plan_desc *plan, const int64_t *vertex, const int32_t *edge, int32_t v_cnt,
-                             int64_t stride, int threads, double max_seconds, uint64_t *raw_sum, int64_t *processed);
+                             int64_t stride, int64_t offset, int threads, double max_seconds, uint64_t *raw_sum,
+                             int64_t *processed);
 
 /* Independent brute force: number of subgraphs of the graph isomorphic to
  * the n-vertex pattern adj (n*n '0'/'1'), edge-induced (induced = 0) or

@@ -36,8 +36,8 @@ def lib():
         L.oracle_count_timed.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_int,
                                          C.c_double, C.POINTER(C.c_uint64), C.POINTER(C.c_int64)]
         L.oracle_count_edges_timed.restype = C.c_int
-        L.oracle_count_edges_timed.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_int64, C.c_int,
-                                               C.c_double, C.POINTER(C.c_uint64), C.POINTER(C.c_int64)]
+        L.oracle_count_edges_timed.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_int64, C.c_int64,
+                                               C.c_int, C.c_double, C.POINTER(C.c_uint64), C.POINTER(C.c_int64)]
         L.oracle_brute_count.restype = C.c_uint64
         L.oracle_brute_count.argtypes = [C.c_int, C.c_char_p, C.c_int, C.c_void_p, C.c_void_p, C.c_int32]
         L.oracle_clique_count.restype = C.c_uint64
@@ -95,12 +95,13 @@ def count_timed(plan_desc, vertex, edge, stride, max_seconds, threads=0):
     return raw.value, done.value
 
 
-def count_edges_timed(plan_desc, vertex, edge, stride, max_seconds=0.0, threads=0):
-    """(raw sum, edges counted) over every stride-th directed edge."""
+def count_edges_timed(plan_desc, vertex, edge, stride, max_seconds=0.0, threads=0, offset=0):
+    """(raw sum, edges counted) over the directed edges offset, offset +
+    stride, offset + 2 * stride, ..."""
     vertex, edge = _arrays(vertex, edge)
     raw, done = C.c_uint64(), C.c_int64()
     rc = lib().oracle_count_edges_timed(C.byref(plan_desc), vertex.ctypes.data, edge.ctypes.data, len(vertex) - 1,
-                                        stride, threads, max_seconds, C.byref(raw), C.byref(done))
+                                        stride, offset, threads, max_seconds, C.byref(raw), C.byref(done))
     if rc != 0:
         raise ValueError("oracle_count_edges_timed rejected its input")
     return raw.value, done.value

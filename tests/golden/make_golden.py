@@ -1,10 +1,11 @@
 """Regenerates the golden fixtures in this directory from the reference itself.
 
-Run in a checkout that has the reference sources (default /root/reference)
+Run in a checkout that has the reference sources ($GI_REFERENCE, else a
+"reference" directory beside this repository)
 after ``make -C oracle ref`` has built the reference CPU binaries into
 oracle/_ref/:
 
-    python tests/golden/make_golden.py [--ref /root/reference]
+    python tests/golden/make_golden.py [--ref <reference checkout>]
 
 Writes
   plans.jsonl   every Schedule_IEP field of the reference planner for each job
@@ -24,6 +25,7 @@ from __future__ import annotations
 import argparse
 import hashlib
 import json
+import os
 import re
 import subprocess
 import sys
@@ -240,7 +242,7 @@ def write_fsm():
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("GI_REFERENCE", str(ROOT.parent / "reference")))
     ap.add_argument("--skip-plans", action="store_true")
     ap.add_argument("--only-fsm", action="store_true")
     a = ap.parse_args()

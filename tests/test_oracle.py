@@ -12,7 +12,10 @@ import pytest
 import graphindor_b200 as gi
 from conftest import plan_desc
 
-WIKI = Path("/root/reference/dataset/wiki-vote.g")
+# The reference checkout ($GI_REFERENCE, else "reference" beside this
+# repository); its one shipped dataset, when present.
+REFERENCE = Path(os.environ.get("GI_REFERENCE", str(Path(__file__).resolve().parents[2] / "reference")))
+WIKI = REFERENCE / "dataset" / "wiki-vote.g"
 
 
 def _oracle_count(oracle, g, n, adj, enable_iep=True, tri=0, model=1):
