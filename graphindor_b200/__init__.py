@@ -226,6 +226,8 @@ class Graph:
         self.tri_cnt = info.tri_cnt
         self.max_degree = info.max_degree
         self.max_intersection_size = info.max_intersection_size
+        self.n_hubs = info.n_hubs
+        self.hub_min_degree = info.hub_min_degree
 
     @classmethod
     def from_csr(cls, vertex: np.ndarray, edge: np.ndarray, tri_cnt: int = 0, stream: int = 0) -> "Graph":

@@ -83,7 +83,7 @@ __global__ void __launch_bounds__(kBlockThreads, kMinBlocks)
                      int64_t num_shards, int64_t n_chunks, int64_t perm_a, int64_t perm_b,
                      unsigned long long hard_ns, unsigned long long max_claims, Handoff *hitems,
                      unsigned long long hcap, uint32_t hepoch, uint32_t v_cnt, int64_t edge_step,
-                     int64_t edge_offset) {
+                     int64_t edge_offset, HubIndex hubs) {
     __shared__ WarpState states[kWarpsPerBlock];
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
@@ -95,6 +95,7 @@ __global__ void __launch_bounds__(kBlockThreads, kMinBlocks)
     const unsigned long long t_start = globaltimer();
     c.t_start = t_start;
     c.hard_ns = hard_ns;
+    c.hubs = hubs;
     if (hitems) {
         c.hq.items = hitems;
         c.hq.cap = hcap;
@@ -263,6 +264,18 @@ __global__ void __launch_bounds__(kBlockThreads, kMinBlocks)
 
 }  // namespace
 
+// The graph's hub bitmaps as the DFS reads them (none when it has no hubs).
+HubIndex graph_hubs(const gi_graph *g) {
+    HubIndex h;
+    if (g->n_hubs > 0) {
+        h.bits = g->d_hub_bits;
+        h.row = g->d_hub_row;
+        h.words = g->hub_words;
+        h.min_degree = g->hub_min_degree;
+    }
+    return h;
+}
+
 // Ensures the graph's scratch can hold `bytes`; caller holds g->mu.
 int ensure_scratch(gi_graph *g, size_t bytes) {
     if (g->scratch_bytes >= bytes) return GI_OK;
@@ -429,7 +442,8 @@ int count_impl(gi_graph *g, const DevPlan &P, cudaStream_t st, uint64_t *raw_sum
                                              static_cast<uint32_t *>(g->d_scratch), stride, g->d_counters, budget_ns,
                                              shard, num_shards, n_chunks, perm_a, perm_b, hard_ns, max_claims,
                                              hitems, kHandoffCap, g->handoff_epoch,
-                                             static_cast<uint32_t>(g->v_cnt), edge_step, edge_offset);
+                                             static_cast<uint32_t>(g->v_cnt), edge_step, edge_offset,
+                                             graph_hubs(g));
     launches += 1;
     e = cudaGetLastError();
     cudaEventRecord(t1, st);

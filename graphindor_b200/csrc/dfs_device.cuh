@@ -28,6 +28,7 @@ constexpr int kCounterSlots = 16;
 struct WarpState {
     const uint32_t *set_ptr[GI_MAX_PREFIX];
     int32_t set_size[GI_MAX_PREFIX];
+    int32_t hub[GI_MAX_PREFIX];        // row in the graph's hub bitmaps when the set is a hub's list, else -1
     uint32_t emb_mask[GI_MAX_PREFIX];  // leaf level: which emb[0, D) lie in each earlier set
     uint32_t emb[GI_MAX_PATTERN + 1];
     int32_t cursor[GI_MAX_PATTERN + 1];
@@ -47,6 +48,27 @@ struct Handoff {
     int32_t hi;
     uint32_t ready;  // == the launch's epoch once the item is written
 };
+
+// Adjacency bitmaps of the graph's highest-degree vertices (hubs): row r
+// has bit x set when x is a neighbour of the r-th hub, so a membership test
+// against a hub's list is one load instead of a search.  Every vertex of
+// degree >= min_degree is a hub and row[v] gives its row (row[] is read only
+// for such vertices).  n == 0 (the default): no bitmaps, searches only.
+struct HubIndex {
+    const uint32_t *bits = nullptr;
+    const int32_t *row = nullptr;
+    int64_t words = 0;  // 32-bit words per row
+    int32_t min_degree = 0x7fffffff;
+};
+
+__device__ __forceinline__ bool hub_test(const HubIndex &H, int r, uint32_t x) {
+    return (__ldg(&H.bits[static_cast<int64_t>(r) * H.words + (x >> 5)]) >> (x & 31)) & 1u;
+}
+
+// Row of v's bitmap, or -1 when v (degree deg) is not a hub.
+__device__ __forceinline__ int hub_row_of(const HubIndex &H, uint32_t v, int deg) {
+    return deg >= H.min_degree ? __ldg(&H.row[v]) : -1;
+}
 
 struct HandoffQueue {
     Handoff *items = nullptr;       // nullptr: donation off
@@ -266,6 +288,74 @@ __device__ __forceinline__ void lane_intersect(const uint32_t *a, int na, const 
     below = need_total ? bel : tot;
 }
 
+// One lane: |a ∩ N(h)| and |a ∩ N(h) ∩ [0, bound)| for a hub h (bitmap row
+// r), one bit test per element of a; with need_total false only elements
+// below bound are tested.  Loads are issued four at a time.
+__device__ __forceinline__ void lane_count_hub(const HubIndex &H, int r, const uint32_t *a, int na, uint32_t bound,
+                                               bool need_total, int &total, int &below) {
+    int tot = 0, bel = 0;
+    int i = 0;
+    for (; i + 4 <= na; i += 4) {
+        const uint32_t x0 = a[i], x1 = a[i + 1], x2 = a[i + 2], x3 = a[i + 3];
+        if (!need_total && x0 >= bound) {
+            na = i;  // sorted: nothing further is below bound
+            break;
+        }
+        const bool h0 = hub_test(H, r, x0), h1 = hub_test(H, r, x1), h2 = hub_test(H, r, x2), h3 = hub_test(H, r, x3);
+        tot += h0 + h1 + h2 + h3;
+        bel += (h0 && x0 < bound) + (h1 && x1 < bound) + (h2 && x2 < bound) + (h3 && x3 < bound);
+    }
+    for (; i < na; ++i) {
+        const uint32_t x = a[i];
+        if (!need_total && x >= bound) break;
+        const bool h = hub_test(H, r, x);
+        tot += h;
+        bel += h && x < bound;
+    }
+    total = need_total ? tot : bel;
+    below = bel;
+}
+
+// Warp-cooperative |a ∩ N(h)| and |a ∩ N(h) ∩ [0, bound)| (warp-uniform).
+__device__ __forceinline__ void warp_count_hub(const HubIndex &H, int r, const uint32_t *a, int na, uint32_t bound,
+                                               bool need_total, int lane, int &total, int &below) {
+    if (!need_total) na = lower_bound_u32(a, na, bound);
+    int t = 0, u = 0;
+    for (int i = lane; i < na; i += 32) {
+        const uint32_t x = a[i];
+        if (hub_test(H, r, x)) {
+            ++t;
+            u += x < bound;
+        }
+    }
+    for (int o = 16; o; o >>= 1) {
+        t += __shfl_xor_sync(kFull, t, o);
+        u += __shfl_xor_sync(kFull, u, o);
+    }
+    total = need_total ? t : u;
+    below = u;
+}
+
+// Warp-cooperative a ∩ N(h) written to out in a's (sorted) order, or only
+// its size when out is nullptr.
+__device__ __forceinline__ int warp_intersect_hub(const HubIndex &H, int r, const uint32_t *a, int na, uint32_t *out,
+                                                  int lane) {
+    int count = 0;
+    for (int base = 0; base < na; base += 32) {
+        const int i = base + lane;
+        uint32_t x = 0;
+        bool found = false;
+        if (i < na) {
+            x = a[i];
+            found = hub_test(H, r, x);
+        }
+        const unsigned m = __ballot_sync(kFull, found);
+        if (out && found) out[count + __popc(m & ((1u << lane) - 1u))] = x;
+        count += __popc(m);
+    }
+    return count;
+}
+
 // Steps a lane would spend intersecting lists of sizes x and y: the smaller
 // times the log of the size ratio.
 __device__ __forceinline__ int lane_cost(int x, int y) {
@@ -349,6 +439,7 @@ struct Ctx {
     unsigned long long hard_ns = 0;  // > 0: give up the current work item past this much time
     bool aborted = false;
     HandoffQueue hq{};
+    HubIndex hubs{};
 
     // Offers [lo, hi) of depth d's loop to an idle warp (warp-uniform);
     // true when it was queued and is no longer this warp's to do.
@@ -389,25 +480,37 @@ struct Ctx {
         const int64_t l = __ldg(&vertex[v]);
         const int deg = static_cast<int>(__ldg(&vertex[v + 1]) - l);
         const uint32_t *nb = edge + l;
+        const int hv = hub_row_of(hubs, v, deg);  // v's own bitmap row, or -1
         for (int p = P.last[d]; p != -1; p = P.next[p]) {
             int size;
             const int f = P.father[p];
             if (f == -1) {
-                if (lane == 0) w.set_ptr[p] = nb;
+                if (lane == 0) {
+                    w.set_ptr[p] = nb;
+                    w.hub[p] = hv;
+                }
                 size = deg;
                 if (kBytesOn && account && lane == 0) bytes += 16;
             } else {
                 const uint32_t *fs = w.set_ptr[f];
                 const int fn = w.set_size[f];
-                if (P.mode[p] == kMaterialize) {
-                    uint32_t *out = slot_base + static_cast<int64_t>(P.slot[p]) * slot_stride;
+                const int hf = w.hub[f];
+                // A hub's list on either side: test the other list's elements
+                // against its bitmap.
+                const bool by_f = hf >= 0 && fn >= deg, by_v = !by_f && hv >= 0;
+                uint32_t *out = P.mode[p] == kMaterialize ? slot_base + static_cast<int64_t>(P.slot[p]) * slot_stride
+                                                          : nullptr;
+                if (by_f)
+                    size = warp_intersect_hub(hubs, hf, nb, deg, out, lane);
+                else if (by_v)
+                    size = warp_intersect_hub(hubs, hv, fs, fn, out, lane);
+                else
                     size = warp_intersect(fs, fn, nb, deg, out, lane);
-                    if (lane == 0) w.set_ptr[p] = out;
-                    if (kBytesOn && account && lane == 0) bytes += 4ull * (fn + deg + size);
-                } else {
-                    size = warp_intersect(fs, fn, nb, deg, nullptr, lane);
-                    if (kBytesOn && account && lane == 0) bytes += 4ull * (fn + deg);
+                if (lane == 0) {
+                    if (out) w.set_ptr[p] = out;
+                    w.hub[p] = -1;
                 }
+                if (kBytesOn && account && lane == 0) bytes += 4ull * (fn + deg + (out ? size : 0));
             }
             if (lane == 0) w.set_size[p] = size;
             __syncwarp();
@@ -480,11 +583,15 @@ struct Ctx {
         const int64_t l = __ldg(&vertex[v]);
         const int dv = static_cast<int>(__ldg(&vertex[v + 1]) - l);
         const uint32_t *nv = edge + l;
+        const int hv = hub_row_of(hubs, v, dv);
         uint32_t mask_nv = 0;  // emb[u] in N(v)
         if (kWarp) {
-            mask_nv = __ballot_sync(kFull, lane < D && contains_u32(nv, dv, w.emb[lane]));
+            mask_nv = __ballot_sync(kFull, lane < D && (hv >= 0 ? hub_test(hubs, hv, w.emb[lane])
+                                                              : contains_u32(nv, dv, w.emb[lane])));
         } else {
-            for (int u = 0; u < D; ++u) mask_nv |= static_cast<uint32_t>(contains_u32(nv, dv, w.emb[u])) << u;
+            for (int u = 0; u < D; ++u)
+                mask_nv |= static_cast<uint32_t>(hv >= 0 ? hub_test(hubs, hv, w.emb[u]) : contains_u32(nv, dv, w.emb[u]))
+                           << u;
         }
         const bool count_here = !kWarp || lane == 0;  // who adds the bytes
         const int stop = P.stop;
@@ -514,11 +621,23 @@ struct Ctx {
                 // L's own prune is implied by its count (a set that holds only
                 // embedded vertices counts zero), so L alone may stop at bound.
                 const bool need_total = kBytesOn || !(last_level && p == L);
+                const int hf = w.hub[f];
                 int tot, bel;
-                if (kWarp)
+                if (hf >= 0 && fn >= dv) {
+                    if (kWarp)
+                        warp_count_hub(hubs, hf, nv, dv, bound, need_total, lane, tot, bel);
+                    else
+                        lane_count_hub(hubs, hf, nv, dv, bound, need_total, tot, bel);
+                } else if (hv >= 0) {
+                    if (kWarp)
+                        warp_count_hub(hubs, hv, fs, fn, bound, need_total, lane, tot, bel);
+                    else
+                        lane_count_hub(hubs, hv, fs, fn, bound, need_total, tot, bel);
+                } else if (kWarp) {
                     warp_count2(fs, fn, nv, dv, bound, need_total, lane, tot, bel);
-                else
+                } else {
                     lane_intersect(fs, fn, nv, dv, bound, need_total, tot, bel);
+                }
                 size[p] = tot;
                 if (p == L) below_L = bel;
                 mask[p] = w.emb_mask[f] & mask_nv;
@@ -616,9 +735,15 @@ struct Ctx {
                 for (int u = 0; u < D; ++u) used |= w.emb[u] == v;
                 if (!used && !(P.vertex_induced && anti_adjacent(P, w, D, v, vertex, edge))) {
                     const int dv = static_cast<int>(__ldg(&vertex[v + 1]) - __ldg(&vertex[v]));
+                    const bool v_hub = dv >= hubs.min_degree;
                     int cost = 0;
-                    for (int p = P.last[D]; p != -1; p = P.next[p])
-                        if (P.father[p] >= 0) cost += lane_cost(w.set_size[P.father[p]], dv);
+                    for (int p = P.last[D]; p != -1; p = P.next[p]) {
+                        const int f = P.father[p];
+                        if (f < 0) continue;
+                        const int fn = w.set_size[f];
+                        // bitmap tests: one step per element of the other list
+                        cost += w.hub[f] >= 0 && fn >= dv ? dv : v_hub ? fn : lane_cost(fn, dv);
+                    }
                     heavy = cost > (kLaneBudgetOverride >= 0 ? kLaneBudgetOverride : P.lane_budget);
                     if (!heavy) acc += leaf_eval<false>(D, v);
                 }

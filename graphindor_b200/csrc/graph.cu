@@ -7,7 +7,9 @@
 // (there built on the host at :27-31, here by a kernel).
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdio>
+#include <functional>
 #include <cstring>
 #include <new>
 #include <vector>
@@ -56,7 +58,74 @@ __global__ void build_edge_from_kernel(const int64_t *__restrict__ vertex, const
     }
 }
 
+// Block r: the bitmap row of hub ids[r] (bits zeroed before) and its entry
+// in the row index.
+__global__ void build_hub_bits_kernel(const int64_t *__restrict__ vertex, const int32_t *__restrict__ edge,
+                                      const int32_t *__restrict__ ids, int64_t words, uint32_t *__restrict__ bits,
+                                      int32_t *__restrict__ row) {
+    const int r = blockIdx.x;
+    const int32_t h = ids[r];
+    if (threadIdx.x == 0) row[h] = r;
+    uint32_t *b = bits + static_cast<int64_t>(r) * words;
+    for (int64_t j = vertex[h] + threadIdx.x; j < vertex[h + 1]; j += blockDim.x) {
+        const uint32_t x = static_cast<uint32_t>(edge[j]);
+        atomicOr(&b[x >> 5], 1u << (x & 31));
+    }
+}
+
 }  // namespace
+
+// Hub bitmaps: the counting DFS tests membership in a hub's adjacency list
+// with one load.  Hubs are all vertices of degree >= T, T the smallest value
+// >= kHubMinDegree for which their bitmaps fit kHubBitmapBytes.
+int cuda_fail(cudaError_t e, const char *what);
+
+constexpr size_t kHubBitmapBytes = size_t(64) << 20;
+constexpr int32_t kHubMinDegree = 256;
+
+static int build_hubs(gi_graph *g, const int64_t *vertex, cudaStream_t st) {
+    const int64_t words = (static_cast<int64_t>(g->v_cnt) + 31) / 32;
+    const int64_t max_hubs = static_cast<int64_t>(kHubBitmapBytes / (static_cast<size_t>(words) * sizeof(uint32_t)));
+    if (max_hubs < 1 || g->max_degree < kHubMinDegree) return GI_OK;
+    std::vector<int32_t> big;
+    for (int32_t v = 0; v < g->v_cnt; ++v) {
+        const int64_t d = vertex[v + 1] - vertex[v];
+        if (d >= kHubMinDegree) big.push_back(static_cast<int32_t>(d));
+    }
+    int32_t T = kHubMinDegree;
+    if (static_cast<int64_t>(big.size()) > max_hubs) {
+        std::nth_element(big.begin(), big.begin() + max_hubs, big.end(), std::greater<int32_t>());
+        T = big[static_cast<size_t>(max_hubs)] + 1;  // the (max_hubs+1)-th largest degree is left out
+    }
+    std::vector<int32_t> ids;
+    for (int32_t v = 0; v < g->v_cnt; ++v)
+        if (vertex[v + 1] - vertex[v] >= T) ids.push_back(v);
+    if (ids.empty()) return GI_OK;
+    int32_t *d_ids = nullptr;
+    cudaError_t e;
+    const size_t bits_bytes = ids.size() * static_cast<size_t>(words) * sizeof(uint32_t);
+    if ((e = cudaMalloc(&g->d_hub_bits, bits_bytes)) != cudaSuccess ||
+        (e = cudaMalloc(&g->d_hub_row, sizeof(int32_t) * static_cast<size_t>(g->v_cnt))) != cudaSuccess ||
+        (e = cudaMalloc(&d_ids, sizeof(int32_t) * ids.size())) != cudaSuccess) {
+        cudaFree(d_ids);
+        return cuda_fail(e, "hub bitmap allocation");
+    }
+    if ((e = cudaMemcpyAsync(d_ids, ids.data(), sizeof(int32_t) * ids.size(), cudaMemcpyHostToDevice, st)) ==
+            cudaSuccess &&
+        (e = cudaMemsetAsync(g->d_hub_bits, 0, bits_bytes, st)) == cudaSuccess &&
+        (e = cudaMemsetAsync(g->d_hub_row, 0xff, sizeof(int32_t) * static_cast<size_t>(g->v_cnt), st)) == cudaSuccess) {
+        build_hub_bits_kernel<<<static_cast<unsigned>(ids.size()), 256, 0, st>>>(g->d_vertex, g->d_edge, d_ids, words,
+                                                                               g->d_hub_bits, g->d_hub_row);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);  // d_ids is freed next
+    cudaFree(d_ids);
+    if (e != cudaSuccess) return cuda_fail(e, "hub bitmap build");
+    g->n_hubs = static_cast<int32_t>(ids.size());
+    g->hub_min_degree = T;
+    g->hub_words = words;
+    return GI_OK;
+}
 
 void cost_model_graph_features(const int64_t *vertex, int32_t v_cnt, int64_t tri_cnt, float *out);
 
@@ -108,6 +177,8 @@ void graph_free(gi_graph *g) {
     cudaFree(g->d_bitmap);
     cudaFree(g->d_bitmap_off);
     cudaFree(g->d_roots);
+    cudaFree(g->d_hub_bits);
+    cudaFree(g->d_hub_row);
     cudaSetDevice(prev);
     delete g;
 }
@@ -181,6 +252,11 @@ int graph_create_impl(const int64_t *vertex, const int32_t *edge, int32_t v_cnt,
         graph_free(g);
         return fail(GI_EINVAL, "adjacency lists must be sorted, duplicate-free, in range and without self-loops");
     }
+    const int hub_status = build_hubs(g, vertex, st);
+    if (hub_status != GI_OK) {
+        graph_free(g);
+        return hub_status;
+    }
     *out = g;
     return GI_OK;
 }
@@ -208,6 +284,8 @@ int gi_graph_get_info(const gi_graph *g, gi_graph_info *o) {
     o->tri_cnt = g->tri_cnt;
     o->max_degree = g->max_degree;
     o->max_intersection_size = g->max_isect;
+    o->n_hubs = g->n_hubs;
+    o->hub_min_degree = g->hub_min_degree;
     return GI_OK;
 }
 

@@ -140,4 +140,12 @@ struct gi_graph {
     // Roots of the clique-tree pivoting search, largest out-degree first
     // (kclique.cu), built with the bitmaps' first pivoting count and kept.
     int32_t *d_roots = nullptr;
+    // Adjacency bitmaps of the hubs (every vertex of degree >= hub_min_degree;
+    // graph.cu): n_hubs rows of hub_words 32-bit words, and hub_row[v] = the
+    // row of hub v (-1 for other vertices).  Read by the counting DFS.
+    uint32_t *d_hub_bits = nullptr;
+    int32_t *d_hub_row = nullptr;
+    int32_t n_hubs = 0;
+    int32_t hub_min_degree = 0x7fffffff;
+    int64_t hub_words = 0;
 };

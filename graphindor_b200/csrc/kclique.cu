@@ -448,9 +448,9 @@ int kclique_pivot(gi_graph *o, int kmax, cudaStream_t st, uint64_t *counts, gi_s
     const int64_t max_levels = L.dmax + 2;
     L.levels = std::min<int64_t>(64, max_levels);
     // Roots by out-degree, largest first (counting sort on the host; ties in
-    // id order).
-    int32_t *d_roots = nullptr;
-    {
+    // id order), built once and kept on the DAG next to its bitmaps.
+    if (!o->d_roots) {
+        int32_t *d_roots = nullptr;
         std::vector<int64_t> hv(static_cast<size_t>(o->v_cnt) + 1);
         cudaError_t e = cudaMemcpyAsync(hv.data(), o->d_vertex, hv.size() * sizeof(int64_t), cudaMemcpyDeviceToHost, st);
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);
@@ -473,7 +473,9 @@ int kclique_pivot(gi_graph *o, int kmax, cudaStream_t st, uint64_t *counts, gi_s
             cudaFree(d_roots);
             return cuda_fail(e, "root order");
         }
+        o->d_roots = d_roots;
     }
+    const int32_t *d_roots = o->d_roots;
     float total_ms = 0.f;
     while (true) {
         const size_t per_warp = static_cast<size_t>(L.words()) * sizeof(uint32_t);
@@ -514,14 +516,10 @@ int kclique_pivot(gi_graph *o, int kmax, cudaStream_t st, uint64_t *counts, gi_s
         cudaFree(scratch);
         cudaFree(binom);
         cudaFree(ctr);
-        if (e != cudaSuccess) {
-            cudaFree(d_roots);
-            return cuda_fail(e, "clique-tree pivoting kernel");
-        }
+        if (e != cudaSuccess) return cuda_fail(e, "clique-tree pivoting kernel");
         ++launches;
         total_ms += ms;
         if (host[1] == 0) {
-            cudaFree(d_roots);
             counts[0] = 0;
             for (int k = 1; k <= kmax; ++k) counts[k] = host[2 + k];
             if (stats) {
@@ -536,7 +534,6 @@ int kclique_pivot(gi_graph *o, int kmax, cudaStream_t st, uint64_t *counts, gi_s
             return GI_OK;
         }
         if (L.levels >= max_levels) {
-            cudaFree(d_roots);
             return fail(GI_EOVERFLOW, "clique-tree pivoting: search deeper than its stack");
         }
         L.levels = std::min<int64_t>(L.levels * 4, max_levels);

@@ -69,6 +69,10 @@ typedef struct gi_graph_info {
     int64_t tri_cnt;
     int32_t max_degree;
     int32_t max_intersection_size; /* second-largest degree (reference src/dataloader.cpp:297-301) */
+    int32_t n_hubs;                /* vertices whose adjacency the counting kernels test through a
+                                      bitmap: all of degree >= hub_min_degree (their bitmaps are
+                                      held to 64 MiB per graph) */
+    int32_t hub_min_degree;
 } gi_graph_info;
 int gi_graph_get_info(const gi_graph *g, gi_graph_info *out);
 

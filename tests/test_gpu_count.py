@@ -141,6 +141,33 @@ def test_larger_graph_invariants(oracle):
     assert gi.pattern_matching(dg, s4).count == gi.clique_count(dg, 4, 1).count == gi.clique_count(dg, 4, 0).count
 
 
+def test_hub_bitmaps_keep_counts_exact(oracle):
+    """A graph with hubs (vertices whose lists the kernels test through a
+    bitmap): edge subsets of the workload patterns and a 7-vertex pattern,
+    whole counts of the cheaper ones, and the algorithmic bytes, against the
+    oracle.  Both sides of every bitmap path run: hub lists as the father set
+    and hubs as candidates, in the warp-built prefixes and the leaf level."""
+    g = gen.rmat(14, 12.0, 2)
+    dg = gi.Graph.from_csr(g.vertex, g.edge)
+    assert dg.n_hubs > 0 and dg.hub_min_degree >= 256
+    deg = np.diff(g.vertex)
+    assert dg.n_hubs == int((deg >= dg.hub_min_degree).sum())
+    pats = [(4, "0111101111001100"), (4, "0110100110010110"), (5, "0101110101010101010011000"),
+            (5, "0111110111110111110111110"), (6, "011100101010110001100011010101001110"),
+            (6, "010101101000010100101010000101100010"), (7, "0111111101111111011101110100111100011100001100000")]
+    for n, adj in pats:
+        for iep in (True, False):
+            s = gi.Schedule_IEP(gi.Pattern(n, adj), g.v_cnt, g.e_cnt, 0, enable_iep=iep)
+            d = plan_desc(s)
+            want, _ = oracle.count_edges_timed(d, g.vertex, g.edge, 211, offset=17)
+            assert gi.count_edges(dg, s, 211, 17).raw_sum == want, (adj, iep)
+            if n <= 5:
+                raw, nbytes = oracle.count(d, g.vertex, g.edge, want_bytes=True)
+                r = gi.pattern_matching(dg, s, count_bytes=True)
+                assert r.raw_sum == raw and r.alg_bytes == nbytes, (adj, iep)
+                assert gi.pattern_matching(dg, s).raw_sum == raw
+
+
 def test_budget_expiry_returns_timeout_and_device_stays_usable():
     g = gen.rmat(15, 16.0, 9)
     dg = gi.Graph.from_csr(g.vertex, g.edge)
