@@ -34,15 +34,47 @@ struct BatchJob {
     int64_t e_cnt;
     int64_t chunk_begin;  // first chunk of this job in the launch's numbering
     int32_t plan;         // index into the batch's plans
-    int32_t pad;
+    uint32_t v_cnt;
+    HubIndex hubs;        // the graph's hub bitmaps
 };
 
-// Counter slots of a batch: [0] chunk cursor, [1] launch start (min over warps).
+// Counter slots of a batch: [0] chunk cursor, [1] launch start (min over
+// warps), [2, 6) the handoff queue's head, tail, idle and exited warps, [6]
+// set when a handed-off item was lost.
+constexpr int kBatchCounters = 7;
+constexpr unsigned long long kBatchHandoffCap = 1ull << 20;
+
+// The job's plan into the warp's shared slot (when it changed).
+__device__ __forceinline__ void enter_job(const DevPlan *__restrict__ plans, const BatchJob &J, int job, int &cur,
+                                          DevPlan &P, int lane) {
+    if (job == cur) return;
+    const int32_t *src = reinterpret_cast<const int32_t *>(&plans[J.plan]);
+    int32_t *dst = reinterpret_cast<int32_t *>(&P);
+    for (int i = lane; i < static_cast<int>(sizeof(DevPlan) / 4); i += 32) dst[i] = src[i];
+    __syncwarp();
+    cur = job;
+}
+
+// Advances the handoff queue's epoch before each run (captured in the batch's
+// CUDA graph, so every replay gets a new one): items published by an earlier
+// run never look ready to this one.
+__global__ void bump_epoch_kernel(uint32_t *epoch) {
+    uint32_t x = *epoch + 1;
+    if (x == 0) x = 1;
+    *epoch = x;
+}
+
+// One of a job's work items is done: the last one records the job's end time.
+__device__ __forceinline__ void job_item_done(unsigned long long *job_left, unsigned long long *job_done, int job) {
+    if (atomicAdd(&job_left[job], ~0ull) == 1ull) job_done[job] = globaltimer();
+}
+
 __global__ void __launch_bounds__(kBlockThreads)
     batch_count_kernel(const DevPlan *__restrict__ plans, const BatchJob *__restrict__ jobs, int n_jobs,
                        int64_t total_chunks, uint32_t *scratch, int64_t slot_stride, int64_t slots_per_warp,
                        unsigned long long *counters, unsigned long long *job_sum, unsigned long long *job_left,
-                       unsigned long long *job_done) {
+                       unsigned long long *job_done, Handoff *hitems, unsigned long long hcap,
+                       const uint32_t *hepoch) {
     __shared__ WarpState states[kWarpsPerBlock];
     __shared__ DevPlan plan_s[kWarpsPerBlock];
     const int lane = threadIdx.x & 31;
@@ -52,6 +84,14 @@ __global__ void __launch_bounds__(kBlockThreads)
     DevPlan &P = plan_s[wib];
     uint32_t *slots = scratch + gwarp * slots_per_warp * slot_stride;
     if (lane == 0) atomicMin(&counters[1], globaltimer());
+    HandoffQueue hq;
+    if (hitems) {
+        hq.items = hitems;
+        hq.cap = hcap;
+        hq.ctr = counters + 2;
+        hq.epoch = *hepoch;
+        hq.job_left = job_left;
+    }
     int cur = -1;
     while (true) {
         unsigned long long c = 0;
@@ -69,14 +109,12 @@ __global__ void __launch_bounds__(kBlockThreads)
         }
         const int job = lo;
         const BatchJob J = jobs[job];
-        if (job != cur) {
-            const int32_t *src = reinterpret_cast<const int32_t *>(&plans[J.plan]);
-            int32_t *dst = reinterpret_cast<int32_t *>(&P);
-            for (int i = lane; i < static_cast<int>(sizeof(DevPlan) / 4); i += 32) dst[i] = src[i];
-            __syncwarp();
-            cur = job;
-        }
+        enter_job(plans, J, job, cur, P, lane);
         Ctx<false> ctx{P, J.vertex, J.edge, slots, slot_stride, w, lane, 0ull};
+        ctx.hubs = J.hubs;
+        ctx.hq = hq;
+        ctx.hq.job = job;
+        ctx.hq.v_cnt = J.v_cnt;
         const int64_t e = (static_cast<int64_t>(c) - J.chunk_begin) * kTaskChunk + lane;
         bool valid = e < J.e_cnt;
         uint32_t v0 = 0, v1 = 0;
@@ -88,6 +126,11 @@ __global__ void __launch_bounds__(kBlockThreads)
         }
         unsigned todo = __ballot_sync(kFull, valid);
         unsigned long long chunk_sum = 0;
+        if (P.flat_first) {
+            unsigned long long passed = 0;
+            chunk_sum = ctx.first_level_flat(v0, v1, valid, passed);
+            todo = 0;
+        }
         while (todo) {
             const int src = __ffs(todo) - 1;
             todo &= todo - 1;
@@ -104,8 +147,32 @@ __global__ void __launch_bounds__(kBlockThreads)
         }
         if (lane == 0) {
             if (chunk_sum) atomicAdd(&job_sum[job], chunk_sum);
-            if (atomicAdd(&job_left[job], ~0ull) == 1ull) job_done[job] = globaltimer();
+            job_item_done(job_left, job_done, job);
         }
+    }
+    // Out of chunks: ranges other warps handed off, each counted for its own
+    // job (take_handoffs).
+    if (hitems) {
+        const bool lost = take_handoffs(hq, false, lane, [&](long long slot) {
+            const Handoff *h = &hitems[slot];
+            const int job = __ldcg(&h->job);
+            if (job < 0 || job >= n_jobs) return false;
+            const BatchJob J = jobs[job];
+            enter_job(plans, J, job, cur, P, lane);
+            Ctx<false> ctx{P, J.vertex, J.edge, slots, slot_stride, w, lane, 0ull};
+            ctx.hubs = J.hubs;
+            ctx.hq = hq;
+            ctx.hq.job = job;
+            ctx.hq.v_cnt = J.v_cnt;
+            unsigned long long part = 0;
+            const bool ok = ctx.run_handoff(h, part);
+            if (lane == 0) {
+                if (part) atomicAdd(&job_sum[job], part);
+                job_item_done(job_left, job_done, job);
+            }
+            return ok;
+        });
+        if (lost && lane == 0) atomicExch(&counters[6], 1ull);
     }
 }
 
@@ -125,7 +192,9 @@ struct gi_batch {
     DevPlan *d_plans = nullptr;
     BatchJob *d_jobs = nullptr;
     uint32_t *d_scratch = nullptr;
-    unsigned long long *d_ctr = nullptr;  // counters[2] | sum[n] | left[n] | done[n]
+    unsigned long long *d_ctr = nullptr;  // counters[kBatchCounters] | sum[n] | left[n] | done[n]
+    Handoff *d_handoff = nullptr;         // work donation between the batch's warps
+    uint32_t *d_epoch = nullptr;          // the queue's epoch, advanced by every run
     unsigned long long *d_init = nullptr; // the values a run starts from (copied in the graph)
     int64_t slot_stride = 1, slots_per_warp = 1;
     int blocks = 0;
@@ -143,6 +212,8 @@ static void batch_free(gi_batch *b) {
     cudaFree(b->d_scratch);
     cudaFree(b->d_ctr);
     cudaFree(b->d_init);
+    cudaFree(b->d_handoff);
+    cudaFree(b->d_epoch);
     delete b;
 }
 
@@ -168,11 +239,11 @@ int gi_batch_create(gi_graph *const *graphs, const gi_plan *const *plans, int n_
         b->graphs.push_back(g);
         b->plans.push_back(p);
         b->divisor.push_back(static_cast<uint64_t>(p->sched->get_count_divisor()));
-        hplans.push_back(p->dev);
+        hplans.push_back(plan_for_graph(p->dev, g->max_degree));
         const int64_t nch = (g->e_cnt + kTaskChunk - 1) / kTaskChunk;
         b->chunks.push_back(static_cast<unsigned long long>(nch));
         hjobs[j] = BatchJob{g->d_vertex, reinterpret_cast<const uint32_t *>(g->d_edge), g->d_edge_from, g->e_cnt,
-                            chunk, j, 0};
+                            chunk, j, static_cast<uint32_t>(g->v_cnt), hubs_of(g)};
         chunk += nch;
         b->slot_stride = std::max<int64_t>(b->slot_stride, g->max_isect);
         b->slots_per_warp = std::max<int64_t>(b->slots_per_warp, p->dev.n_slots);
@@ -186,10 +257,10 @@ int gi_batch_create(gi_graph *const *graphs, const gi_plan *const *plans, int n_
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_count_kernel, kBlockThreads, 0);
     b->blocks = sms * std::max(per_sm, 1);
     const int64_t warps = static_cast<int64_t>(b->blocks) * kWarpsPerBlock;
-    const size_t ctr_words = 2 + 3 * static_cast<size_t>(n_jobs);
+    const size_t ctr_words = kBatchCounters + 3 * static_cast<size_t>(n_jobs);
     std::vector<unsigned long long> init(ctr_words, 0);
     init[1] = ~0ull;  // launch start: min over warps
-    for (int j = 0; j < n_jobs; ++j) init[2 + n_jobs + j] = b->chunks[j];
+    for (int j = 0; j < n_jobs; ++j) init[kBatchCounters + n_jobs + j] = b->chunks[j];
     cudaError_t e;
     if ((e = cudaMalloc(&b->d_plans, sizeof(DevPlan) * n_jobs)) != cudaSuccess ||
         (e = cudaMalloc(&b->d_jobs, sizeof(BatchJob) * n_jobs)) != cudaSuccess ||
@@ -197,6 +268,10 @@ int gi_batch_create(gi_graph *const *graphs, const gi_plan *const *plans, int n_
             cudaSuccess ||
         (e = cudaMalloc(&b->d_ctr, sizeof(unsigned long long) * ctr_words)) != cudaSuccess ||
         (e = cudaMalloc(&b->d_init, sizeof(unsigned long long) * ctr_words)) != cudaSuccess ||
+        (e = cudaMalloc(&b->d_handoff, sizeof(Handoff) * kBatchHandoffCap)) != cudaSuccess ||
+        (e = cudaMemset(b->d_handoff, 0, sizeof(Handoff) * kBatchHandoffCap)) != cudaSuccess ||
+        (e = cudaMalloc(&b->d_epoch, sizeof(uint32_t))) != cudaSuccess ||
+        (e = cudaMemset(b->d_epoch, 0, sizeof(uint32_t))) != cudaSuccess ||
         (e = cudaMemcpy(b->d_plans, hplans.data(), sizeof(DevPlan) * n_jobs, cudaMemcpyHostToDevice)) !=
             cudaSuccess ||
         (e = cudaMemcpy(b->d_jobs, hjobs.data(), sizeof(BatchJob) * n_jobs, cudaMemcpyHostToDevice)) !=
@@ -221,7 +296,7 @@ int gi_batch_run(gi_batch *b, gi_stream stream, uint64_t *counts, double *job_ms
     cudaStream_t cap = st;
     cudaError_t e = cudaSuccess;
     const int n = b->n_jobs;
-    const size_t ctr_words = 2 + 3 * static_cast<size_t>(n);
+    const size_t ctr_words = kBatchCounters + 3 * static_cast<size_t>(n);
     // The run as a CUDA graph: reset the counters, then the one launch.  The
     // legacy default stream cannot be captured, so a private stream carries
     // the capture in that case.
@@ -231,9 +306,11 @@ int gi_batch_run(gi_batch *b, gi_stream stream, uint64_t *counts, double *job_ms
         if ((e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal)) == cudaSuccess) {
             cudaMemcpyAsync(b->d_ctr, b->d_init, sizeof(unsigned long long) * ctr_words, cudaMemcpyDeviceToDevice,
                             cap);
+            bump_epoch_kernel<<<1, 1, 0, cap>>>(b->d_epoch);
             batch_count_kernel<<<b->blocks, kBlockThreads, 0, cap>>>(
                 b->d_plans, b->d_jobs, n, b->total_chunks, b->d_scratch, b->slot_stride, b->slots_per_warp, b->d_ctr,
-                b->d_ctr + 2, b->d_ctr + 2 + n, b->d_ctr + 2 + 2 * n);
+                b->d_ctr + kBatchCounters, b->d_ctr + kBatchCounters + n, b->d_ctr + kBatchCounters + 2 * n,
+                b->d_handoff, kBatchHandoffCap, b->d_epoch);
             e = cudaStreamEndCapture(cap, &b->graph);
         }
         if (e == cudaSuccess) e = cudaGraphInstantiate(&b->exec, b->graph, 0);
@@ -259,12 +336,13 @@ int gi_batch_run(gi_batch *b, gi_stream stream, uint64_t *counts, double *job_ms
     cudaEventDestroy(t1);
     if (prev != b->device) cudaSetDevice(prev);
     if (e != cudaSuccess) return cuda_fail(e, "batch run");
+    if (host[6]) return fail(GI_ECUDA, "a handed-off batch work item was never published");
     const unsigned long long start = host[1];
     for (int j = 0; j < n; ++j) {
-        const uint64_t raw = host[2 + j];
+        const uint64_t raw = host[kBatchCounters + j];
         counts[j] = b->divisor[j] ? raw / b->divisor[j] : raw;
         if (job_ms) {
-            const unsigned long long done = host[2 + 2 * n + j];
+            const unsigned long long done = host[kBatchCounters + 2 * n + j];
             job_ms[j] = b->chunks[j] == 0 || done < start ? 0.0 : (done - start) * 1e-6;
         }
     }

@@ -1,5 +1,6 @@
 // C ABI: status strings, plans and motif enumeration (host only).
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <functional>
 #include <new>
@@ -107,6 +108,13 @@ static int build_dev_plan(const Schedule_IEP &s, DevPlan &d) {
     // (house 11 %, prism 5 %, 6-cycle + chord 4 % faster at 256 than at 2048);
     // plans without one (cliques) prefer the lanes (5-clique 36 % faster at 2048).
     d.lane_budget = d.iep_k > 0 ? 256 : 2048;
+    // Leaf probes spread over the lanes (one element test per lane and step)
+    // instead of one candidate per lane; GI_LEAF_FLAT=0/1 overrides.
+    d.leaf_flat = 0;
+    if (const char *e = std::getenv("GI_LEAF_FLAT")) d.leaf_flat = std::atoi(e) != 0;
+    // A DFS that ends at depth 2 (triangle- and diamond-like plans): the
+    // first-level edges of a chunk are themselves the flat leaf's candidates.
+    d.flat_first = d.leaf_flat && d.stop == 2 && !(d.vertex_induced && anti_edge);
     for (int p = 0; p < GI_MAX_PREFIX; ++p) d.pdepth[p] = p < tp ? s.get_prefix_data(p).back() : -1;
     // Splitting of the depth-2 loop: its set's members are a subset of {0, 1}.
     d.loop2_kind = -1;

@@ -70,8 +70,6 @@ __global__ void split_count_kernel(const __grid_constant__ DevPlan P, const int6
 // of dependent loads and gain from the extra resident warps despite some
 // spilling (R-MAT scale 22: prism 1.6x, 6-cycle+chord 1.6x faster at 16
 // blocks); shallower plans run best with the unconstrained allocation.
-constexpr unsigned kTakerSpins = 1u << 20;  // empty polls of ~2 us before an idle warp leaves
-constexpr unsigned kReadySpins = 1u << 22;  // polls of a claimed item's ready flag
 constexpr unsigned long long kHandoffCap = 1ull << 20;
 
 template <bool kBytesOn, int kMinBlocks>
@@ -158,6 +156,11 @@ __global__ void __launch_bounds__(kBlockThreads, kMinBlocks)
         }
         unsigned todo = __ballot_sync(kFull, valid);
         unsigned long long chunk_sum = 0, chunk_tasks = 0;
+        if (P.flat_first) {
+            // The DFS ends at depth 2: the chunk's edges are one flat leaf.
+            chunk_sum = c.first_level_flat(v0, v1, valid, chunk_tasks);
+            todo = 0;
+        }
         while (todo) {
             const int src = __ffs(todo) - 1;
             todo &= todo - 1;
@@ -193,64 +196,16 @@ __global__ void __launch_bounds__(kBlockThreads, kMinBlocks)
         tasks += chunk_tasks;
         ++chunks;
     }
-    // Out of chunks: take handed-off ranges until every warp is idle or gone
-    // and the queue is empty.  Waits are bounded: an idle warp gives up after
-    // kTakerSpins empty polls (items still queued then are drained by the
-    // warps that queued them, which poll before they leave), and a taken item
-    // whose ready flag never appears is recorded in kLost.
+    // Out of chunks: take handed-off ranges (take_handoffs).
     bool lost = false;
     const bool warp_timed_out = __shfl_sync(kFull, timed_out ? 1 : 0, 0) != 0;
-    if (hitems && warp_timed_out && lane == 0) atomicAdd(&counters[kQueue + 3], 1ull);  // gone
-    if (hitems && !warp_timed_out) {
-        unsigned long long *qc = counters + kQueue;  // head, tail, idle, exited
-        const unsigned long long total = static_cast<unsigned long long>(gridDim.x) * kWarpsPerBlock;
-        if (lane == 0) atomicAdd(&qc[2], 1ull);
-        unsigned spins = 0;
-        while (true) {
-            long long slot = -1;
-            int quit = 0;
-            if (lane == 0) {
-                const unsigned long long h = *(volatile unsigned long long *)&qc[0];
-                const unsigned long long t = *(volatile unsigned long long *)&qc[1];
-                if (h < (t < hcap ? t : hcap)) {
-                    atomicAdd(&qc[2], ~0ull);  // busy unless the claim fails
-                    if (atomicCAS(&qc[0], h, h + 1) == h)
-                        slot = static_cast<long long>(h);
-                    else
-                        atomicAdd(&qc[2], 1ull);
-                } else {
-                    const unsigned long long idle = *(volatile unsigned long long *)&qc[2];
-                    const unsigned long long gone = *(volatile unsigned long long *)&qc[3];
-                    if (idle + gone >= total || ++spins > kTakerSpins)
-                        quit = 1;
-                    else
-                        __nanosleep(2000);
-                }
-            }
-            slot = __shfl_sync(kFull, slot, 0);
-            if (__shfl_sync(kFull, quit, 0)) break;
-            if (slot < 0) continue;
-            int ready = 0;
-            if (lane == 0) {
-                for (unsigned k = 0; k < kReadySpins && !ready; ++k) {
-                    ready = *(volatile uint32_t *)&hitems[slot].ready == hepoch;
-                    if (!ready) __nanosleep(64);
-                }
-                __threadfence();
-            }
+    if (hitems)
+        lost = take_handoffs(c.hq, warp_timed_out, lane, [&](long long slot) {
             unsigned long long part = 0;
-            if (__shfl_sync(kFull, ready, 0) && slot < static_cast<long long>(hcap) && c.run_handoff(&hitems[slot], part))
-                sum += part;
-            else
-                lost = true;
-            if (lane == 0) atomicAdd(&qc[2], 1ull);
-            spins = 0;
-        }
-        if (lane == 0) {
-            atomicAdd(&qc[2], ~0ull);
-            atomicAdd(&qc[3], 1ull);
-        }
-    }
+            if (!c.run_handoff(&hitems[slot], part)) return false;
+            sum += part;
+            return true;
+        });
     const unsigned long long lane_bytes = kBytesOn ? warp_sum(c.bytes) : 0;
     if (lane == 0) {
         if (lost) atomicAdd(&counters[kLost], 1ull);
@@ -263,18 +218,6 @@ __global__ void __launch_bounds__(kBlockThreads, kMinBlocks)
 }
 
 }  // namespace
-
-// The graph's hub bitmaps as the DFS reads them (none when it has no hubs).
-HubIndex graph_hubs(const gi_graph *g) {
-    HubIndex h;
-    if (g->n_hubs > 0) {
-        h.bits = g->d_hub_bits;
-        h.row = g->d_hub_row;
-        h.words = g->hub_words;
-        h.min_degree = g->hub_min_degree;
-    }
-    return h;
-}
 
 // Ensures the graph's scratch can hold `bytes`; caller holds g->mu.
 int ensure_scratch(gi_graph *g, size_t bytes) {
@@ -354,9 +297,10 @@ DfsKernel pick_dfs_kernel(bool bytes_on, int n) {
 
 // Runs the counting kernel for one plan on one graph (or one shard of it).
 // budget_ms = 0 means no budget.
-int count_impl(gi_graph *g, const DevPlan &P, cudaStream_t st, uint64_t *raw_sum, gi_stats *stats,
+int count_impl(gi_graph *g, const DevPlan &plan, cudaStream_t st, uint64_t *raw_sum, gi_stats *stats,
                double budget_ms, int64_t shard, int64_t num_shards) {
     DeviceGuard device(g->device);
+    const DevPlan P = plan_for_graph(plan, g->max_degree);
     int sms = 148, blocks_per_sm = 1;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, g->device);
     const bool bytes_on = stats && stats->count_bytes;
@@ -443,7 +387,7 @@ int count_impl(gi_graph *g, const DevPlan &P, cudaStream_t st, uint64_t *raw_sum
                                              shard, num_shards, n_chunks, perm_a, perm_b, hard_ns, max_claims,
                                              hitems, kHandoffCap, g->handoff_epoch,
                                              static_cast<uint32_t>(g->v_cnt), edge_step, edge_offset,
-                                             graph_hubs(g));
+                                             hubs_of(g));
     launches += 1;
     e = cudaGetLastError();
     cudaEventRecord(t1, st);

@@ -46,6 +46,7 @@ struct Handoff {
     int32_t depth;
     int32_t lo;
     int32_t hi;
+    int32_t job;     // the batch job the range belongs to (0 for single counts)
     uint32_t ready;  // == the launch's epoch once the item is written
 };
 
@@ -60,6 +61,18 @@ struct HubIndex {
     int64_t words = 0;  // 32-bit words per row
     int32_t min_degree = 0x7fffffff;
 };
+
+// The graph's hub bitmaps as the DFS reads them (none when it has no hubs).
+inline HubIndex hubs_of(const gi_graph *g) {
+    HubIndex h;
+    if (g->n_hubs > 0) {
+        h.bits = g->d_hub_bits;
+        h.row = g->d_hub_row;
+        h.words = g->hub_words;
+        h.min_degree = g->hub_min_degree;
+    }
+    return h;
+}
 
 __device__ __forceinline__ bool hub_test(const HubIndex &H, int r, uint32_t x) {
     return (__ldg(&H.bits[static_cast<int64_t>(r) * H.words + (x >> 5)]) >> (x & 31)) & 1u;
@@ -76,6 +89,8 @@ struct HandoffQueue {
     unsigned long long *ctr = nullptr;  // [0] head, [1] tail, [2] idle warps, [3] exited warps
     uint32_t epoch = 0;
     uint32_t v_cnt = 0;  // items naming a vertex >= v_cnt are rejected
+    int32_t job = 0;     // batches: the job being counted, and its count of
+    unsigned long long *job_left = nullptr;  // outstanding work items (a donation adds one)
 };
 
 // Smallest ranges worth handing off: leaf candidates (lane-parallel) and
@@ -425,6 +440,87 @@ __device__ __forceinline__ unsigned long long iep_combine(const DevPlan &P, cons
     return acc;
 }
 
+// Per lane: |a ∩ b| and |a ∩ b ∩ [0, bound)| for the lane's own pair of
+// sorted lists, with the work of all 32 pairs spread evenly over the lanes.
+// Each lane's probes are the elements of one list of its pair, tested for
+// membership in the other: through a hub's bitmap row when either list is a
+// hub's (ha / hb >= 0; one load per probe), else by binary search of the
+// smaller list's elements in the larger one.  The warp walks the
+// concatenation of all lanes' probes 32 at a time: a lane finds the pair
+// owning its probe (binary search over the exclusive scan of the probe
+// counts), tests it, and the hit ballots are split back to the owners by
+// their probe ranges.  Every lane does one test per step whatever the list
+// sizes, and consecutive lanes read consecutive elements of a list.  Without
+// need_total only elements below bound are probed (tot == bel).  A lane with
+// active false has no probes and gets 0.  All lanes must call it together.
+__device__ __forceinline__ void flat_count(const HubIndex &H, const uint32_t *a, int na, int ha, const uint32_t *b,
+                                           int nb, int hb, uint32_t bound, bool need_total, bool active, int lane,
+                                           int &tot, int &bel) {
+    const uint32_t *probe = a, *tgt = b;
+    int n = 0, tn = -1;  // tn < 0: tgt is a bitmap row
+    if (active) {
+        if (ha >= 0 && na >= nb) {
+            probe = b;
+            n = nb;
+            tgt = H.bits + static_cast<int64_t>(ha) * H.words;
+        } else if (hb >= 0) {
+            probe = a;
+            n = na;
+            tgt = H.bits + static_cast<int64_t>(hb) * H.words;
+        } else if (na <= nb) {
+            probe = a;
+            n = na;
+            tgt = b;
+            tn = nb;
+        } else {
+            probe = b;
+            n = nb;
+            tgt = a;
+            tn = na;
+        }
+        if (!need_total) n = lower_bound_u32(probe, n, bound);
+    }
+    int incl = n;
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(kFull, incl, o);
+        if (lane >= o) incl += y;
+    }
+    const int off = incl - n;
+    const int total = __shfl_sync(kFull, incl, 31);
+    const unsigned long long pa = reinterpret_cast<unsigned long long>(probe);
+    const unsigned long long ta = reinterpret_cast<unsigned long long>(tgt);
+    int t = 0, u = 0;
+    for (int t0 = 0; t0 < total; t0 += 32) {
+        const int item = t0 + lane;
+        // Owner: the last lane whose probes start at or before item.
+        int c = 0;
+        for (int step = 16; step; step >>= 1) {
+            const int o2 = __shfl_sync(kFull, off, c + step);
+            if (o2 <= item) c += step;
+        }
+        const int k = item - __shfl_sync(kFull, off, c);
+        const uint32_t *pc = reinterpret_cast<const uint32_t *>(__shfl_sync(kFull, pa, c));
+        const uint32_t *tc = reinterpret_cast<const uint32_t *>(__shfl_sync(kFull, ta, c));
+        const int tnc = __shfl_sync(kFull, tn, c);
+        const uint32_t bc = __shfl_sync(kFull, bound, c);
+        bool hit = false, below = false;
+        if (item < total) {
+            const uint32_t x = pc[k];
+            hit = tnc < 0 ? ((__ldg(&tc[x >> 5]) >> (x & 31)) & 1u) != 0 : contains_u32(tc, tnc, x);
+            below = hit && x < bc;
+        }
+        const unsigned hm = __ballot_sync(kFull, hit), bm = __ballot_sync(kFull, below);
+        const int lo = max(off - t0, 0), hi = min(off + n - t0, 32);
+        if (lo < hi) {
+            const unsigned rm = (hi == 32 ? kFull : (1u << hi) - 1u) & ~((1u << lo) - 1u);
+            t += __popc(hm & rm);
+            u += __popc(bm & rm);
+        }
+    }
+    tot = t;
+    bel = u;
+}
+
 template <bool kBytesOn>
 struct Ctx {
     const DevPlan &P;
@@ -454,6 +550,8 @@ struct Ctx {
                 h.depth = d;
                 h.lo = lo;
                 h.hi = hi;
+                h.job = hq.job;
+                if (hq.job_left) atomicAdd(&hq.job_left[hq.job], 1ull);
                 __threadfence();
                 *(volatile uint32_t *)&h.ready = hq.epoch;
                 ok = 1;
@@ -759,6 +857,205 @@ struct Ctx {
         return warp_sum(acc);
     }
 
+    // One candidate per lane at the leaf-parent depth D, the probes of all
+    // 32 candidates' intersections spread evenly over the lanes (flat_count).
+    // For each prefix p of D's chain, in chain order (so the break-size prune
+    // still skips later prefixes), every live lane's pair (S_father(p), N(v))
+    // is counted at once; then each lane closes its candidate with the
+    // last-level count or the IEP formula.  `early` describes the sets built
+    // before depth D and the embedding emb[0, D) for this lane: warp-shared
+    // for D >= 2 (EarlyShared), the lane's own first-level edge for D = 1
+    // (EarlyEdge).  The counts, prunes and byte accounting are those of
+    // leaf_eval; so is the result.  Returns this lane's contribution; `passed`
+    // tells whether the candidate passed its chain's break-size prunes.
+    template <class Early>
+    __device__ __forceinline__ unsigned long long flat_eval(int D, uint32_t v, bool alive, const Early &early,
+                                                           bool &passed) {
+        const int stop = P.stop;
+        const int L = P.loop_set[stop];
+        const bool last_level = P.iep_k == 0;
+        int64_t l = 0;
+        int dv = 0, hv = -1;
+        uint32_t bound = 0xffffffffu, mask_nv = 0;
+        if (alive) {
+            l = __ldg(&vertex[v]);
+            dv = static_cast<int>(__ldg(&vertex[v + 1]) - l);
+            hv = hub_row_of(hubs, v, dv);
+            if (last_level)
+                for (int r = P.restrict_last[stop]; r != -1; r = P.restrict_next[r]) {
+                    const int idx = P.restrict_index[r];
+                    bound = min(bound, idx == D ? v : early.emb(idx));
+                }
+            for (int u = 0; u < D; ++u) {
+                const uint32_t x = early.emb(u);
+                mask_nv |= static_cast<uint32_t>(hv >= 0 ? hub_test(hubs, hv, x) : contains_u32(edge + l, dv, x)) << u;
+            }
+        }
+        const uint32_t *nv = edge + l;
+        int size[GI_MAX_PREFIX];
+        uint32_t mask[GI_MAX_PREFIX];
+        int below_L = 0;
+        unsigned long long b = 0;
+        for (int p = P.last[D]; p != -1; p = P.next[p]) {
+            const int f = P.father[p];
+            if (f == -1) {
+                size[p] = dv;
+                mask[p] = mask_nv;
+                if (kBytesOn && alive) b += 16;
+                if (p == L && alive) below_L = lower_bound_u32(nv, dv, bound);
+                if (alive && dv == P.break_size[p]) {
+                    if (kBytesOn) bytes += b;
+                    alive = false;
+                }
+                continue;
+            }
+            const uint32_t *fs = early.set_ptr(f);
+            const int fn = early.set_size(f);
+            const bool need_total = kBytesOn || !(last_level && p == L);
+            int tot, bel;
+            flat_count(hubs, fs, fn, early.hub(f), nv, dv, hv, bound, need_total, alive, lane, tot, bel);
+            size[p] = tot;
+            if (p == L) below_L = bel;
+            mask[p] = early.emb_mask(f) & mask_nv;
+            if (kBytesOn && alive) b += 4ull * (fn + dv + (P.mode[p] == kSizeOnly ? 0 : tot));
+            if (alive && need_total && tot == P.break_size[p]) {
+                if (kBytesOn) bytes += b;
+                alive = false;
+            }
+        }
+        passed = alive;
+        if (!alive) return 0;
+        unsigned long long contrib = 0;
+        if (last_level) {
+            int below;
+            uint32_t m;
+            bool v_in = false;
+            if (P.pdepth[L] == D) {
+                below = below_L;
+                m = mask[L];
+            } else {
+                const uint32_t *sl = early.set_ptr(L);
+                const int nl = early.set_size(L);
+                if (nl <= 0) {
+                    if (kBytesOn) bytes += b;
+                    return 0;
+                }
+                below = lower_bound_u32(sl, nl, bound);
+                m = early.emb_mask(L);
+                v_in = v < bound && contains_u32(sl, below, v);
+            }
+            if (kBytesOn) b += 4ull * below;
+            int emb_below = v_in ? 1 : 0;
+            for (int u = 0; u < D; ++u) emb_below += ((m >> u) & 1u) && early.emb(u) < bound;
+            contrib = static_cast<unsigned long long>(below - emb_below);
+        } else {
+            const int ls_size = P.pdepth[L] == D ? size[L] : early.set_size(L);
+            if (ls_size > 0) {
+                int ans[GI_MAX_IEP_SETS];
+#pragma unroll 1
+                for (int j = 0; j < P.iep_nsets; ++j) {
+                    const int q = P.iep_set[j];
+                    const bool in_chain = P.pdepth[q] == D;
+                    const int sz = in_chain ? size[q] : early.set_size(q);
+                    if (P.iep_set_flag[j]) {
+                        ans[j] = sz - P.iep_set_coef[j];
+                    } else {
+                        const uint32_t m = in_chain ? mask[q] : early.emb_mask(q);
+                        int cnt = __popc(m & ((1u << D) - 1u));
+                        if (!in_chain && contains_u32(early.set_ptr(q), sz, v)) ++cnt;
+                        ans[j] = sz - cnt;
+                        if (kBytesOn) b += 4ull * sz;
+                    }
+                }
+                contrib = iep_combine(P, ans);
+            }
+        }
+        if (kBytesOn) bytes += b;
+        return contrib;
+    }
+
+    // The sets built before the leaf-parent depth, shared by the warp.
+    struct EarlyShared {
+        const WarpState &w;
+        __device__ __forceinline__ uint32_t emb(int u) const { return w.emb[u]; }
+        __device__ __forceinline__ const uint32_t *set_ptr(int q) const { return w.set_ptr[q]; }
+        __device__ __forceinline__ int set_size(int q) const { return w.set_size[q]; }
+        __device__ __forceinline__ int hub(int q) const { return w.hub[q]; }
+        __device__ __forceinline__ uint32_t emb_mask(int q) const { return w.emb_mask[q]; }
+    };
+
+    // Leaf-parent depth D >= 2, 32 candidates of the loop set at a time
+    // (flat_eval).  Returns the warp's sum.
+    __device__ unsigned long long leaf_level_flat(int D, int i0, int i1) {
+        const int ls = P.loop_set[D];
+        const uint32_t *s = w.set_ptr[ls];
+        const int ns = w.set_size[ls];
+        i1 = min(i1, lower_bound_u32(s, ns, w.minv[D]));
+        if (i0 >= i1) return 0;
+        for (int q = 0; q < P.total_prefix; ++q) {
+            if (P.pdepth[q] >= D) continue;
+            const uint32_t m = warp_embedded_mask(w.set_ptr[q], w.set_size[q], w, D, lane);
+            if (lane == 0) w.emb_mask[q] = m;
+        }
+        __syncwarp();
+        const EarlyShared early{w};
+        unsigned long long acc = 0;
+        for (int base = i0; base < i1; base += 32) {
+            if (out_of_time()) break;
+            if (hq.items && i1 - base >= 2 * kLeafHandoffMin) {
+                const int mid = base + ((i1 - base) / 2 + 31) / 32 * 32;
+                if (mid < i1 && donate(D, mid, i1)) i1 = mid;
+            }
+            const int i = base + lane;
+            uint32_t v = 0;
+            bool alive = false;
+            if (i < i1) {
+                v = s[i];
+                bool used = false;
+                for (int u = 0; u < D; ++u) used |= w.emb[u] == v;
+                alive = !used && !(P.vertex_induced && anti_adjacent(P, w, D, v, vertex, edge));
+            }
+            bool passed;
+            acc += flat_eval(D, v, alive, early, passed);
+        }
+        return warp_sum(acc);
+    }
+
+    // The sets of depth 0 for a lane's own first-level edge (v0, v1): every
+    // depth-0 prefix is N(v0), which holds v1 and not v0.
+    struct EarlyEdge {
+        uint32_t v0;
+        const uint32_t *n0;
+        int d0, h0;
+        __device__ __forceinline__ uint32_t emb(int) const { return v0; }
+        __device__ __forceinline__ const uint32_t *set_ptr(int) const { return n0; }
+        __device__ __forceinline__ int set_size(int) const { return d0; }
+        __device__ __forceinline__ int hub(int) const { return h0; }
+        __device__ __forceinline__ uint32_t emb_mask(int) const { return 0u; }
+    };
+
+    // Plans whose DFS ends at depth 2 (P.flat_first): the 32 first-level
+    // edges of a chunk, one per lane, evaluated as leaf candidates v1 at
+    // depth 1 below their own v0 (flat_eval).  Returns the warp's sum;
+    // `passed` counts the edges that passed the depth-1 prunes.
+    __device__ unsigned long long first_level_flat(uint32_t v0, uint32_t v1, bool valid, unsigned long long &passed) {
+        EarlyEdge early{v0, edge, 0, -1};
+        if (valid) {
+            const int64_t l0 = __ldg(&vertex[v0]);
+            early.n0 = edge + l0;
+            early.d0 = static_cast<int>(__ldg(&vertex[v0 + 1]) - l0);
+            early.h0 = hub_row_of(hubs, v0, early.d0);
+        }
+        bool ok = false;
+        const unsigned long long c = flat_eval(1, v1, valid, early, ok);
+        passed = __popc(__ballot_sync(kFull, ok));
+        return warp_sum(c);
+    }
+
+    __device__ __forceinline__ unsigned long long leaf_run(int D, int i0, int i1) {
+        return P.leaf_flat ? leaf_level_flat(D, i0, i1) : leaf_level(D, i0, i1);
+    }
+
     // The DFS below the first two positions for depth-2 candidates [lo, hi);
     // returns the subtask's sum (warp-uniform).
     __device__ unsigned long long dfs(int lo, int hi) { return dfs_from(2, lo, hi); }
@@ -775,7 +1072,7 @@ struct Ctx {
             w.minv[base] = min_vertex(base);
         }
         __syncwarp();
-        if (leaf == base) return leaf_level(base, lo, hi);
+        if (leaf == base) return leaf_run(base, lo, hi);
         int d = base;
         while (true) {
             if (out_of_time()) break;
@@ -786,7 +1083,7 @@ struct Ctx {
                 continue;
             }
             if (d == leaf) {
-                acc += leaf_level(d, 0, 0x7fffffff);
+                acc += leaf_run(d, 0, 0x7fffffff);
                 --d;
                 if (d < base) break;
                 continue;
@@ -861,6 +1158,71 @@ struct Ctx {
         return true;
     }
 };
+
+constexpr unsigned kTakerSpins = 1u << 20;  // empty polls of ~2 us before an idle warp leaves
+constexpr unsigned kReadySpins = 1u << 22;  // polls of a claimed item's ready flag
+
+// A warp out of chunks takes handed-off ranges from hq until every warp is
+// idle or gone and the queue is empty; run(slot) counts item `slot` (its
+// ready flag seen) and returns false when the item fails its checks.  Waits
+// are bounded: an idle warp gives up after kTakerSpins empty polls (items
+// still queued then are drained by the warps that queued them, which poll
+// before they leave), and a taken item whose ready flag never appears is
+// reported.  A warp that timed out only marks itself gone.  Returns true
+// when an item was lost (never published, or rejected).
+template <class Run>
+__device__ bool take_handoffs(const HandoffQueue &hq, bool timed_out, int lane, Run &&run) {
+    unsigned long long *qc = hq.ctr;  // head, tail, idle, exited
+    if (timed_out) {
+        if (lane == 0) atomicAdd(&qc[3], 1ull);  // gone
+        return false;
+    }
+    bool lost = false;
+    const unsigned long long total = static_cast<unsigned long long>(gridDim.x) * kWarpsPerBlock;
+    if (lane == 0) atomicAdd(&qc[2], 1ull);
+    unsigned spins = 0;
+    while (true) {
+        long long slot = -1;
+        int quit = 0;
+        if (lane == 0) {
+            const unsigned long long h = *(volatile unsigned long long *)&qc[0];
+            const unsigned long long t = *(volatile unsigned long long *)&qc[1];
+            if (h < (t < hq.cap ? t : hq.cap)) {
+                atomicAdd(&qc[2], ~0ull);  // busy unless the claim fails
+                if (atomicCAS(&qc[0], h, h + 1) == h)
+                    slot = static_cast<long long>(h);
+                else
+                    atomicAdd(&qc[2], 1ull);
+            } else {
+                const unsigned long long idle = *(volatile unsigned long long *)&qc[2];
+                const unsigned long long gone = *(volatile unsigned long long *)&qc[3];
+                if (idle + gone >= total || ++spins > kTakerSpins)
+                    quit = 1;
+                else
+                    __nanosleep(2000);
+            }
+        }
+        slot = __shfl_sync(kFull, slot, 0);
+        if (__shfl_sync(kFull, quit, 0)) break;
+        if (slot < 0) continue;
+        int ready = 0;
+        if (lane == 0) {
+            for (unsigned k = 0; k < kReadySpins && !ready; ++k) {
+                ready = *(volatile uint32_t *)&hq.items[slot].ready == hq.epoch;
+                if (!ready) __nanosleep(64);
+            }
+            __threadfence();
+        }
+        if (!(__shfl_sync(kFull, ready, 0) && slot < static_cast<long long>(hq.cap) && run(slot))) lost = true;
+        if (lane == 0) atomicAdd(&qc[2], 1ull);
+        spins = 0;
+    }
+    if (lane == 0) {
+        atomicAdd(&qc[2], ~0ull);
+        atomicAdd(&qc[3], 1ull);
+    }
+    return lost;
+}
 
 }  // namespace
 }  // namespace gi

@@ -9,6 +9,7 @@
 
 #include <algorithm>
 #include <cstdio>
+#include <cstdlib>
 #include <functional>
 #include <cstring>
 #include <new>
@@ -83,16 +84,29 @@ int cuda_fail(cudaError_t e, const char *what);
 constexpr size_t kHubBitmapBytes = size_t(64) << 20;
 constexpr int32_t kHubMinDegree = 256;
 
+// The bitmap budget in bytes and the smallest hub degree: the defaults
+// above, or GI_HUB_BITMAP_MB / GI_HUB_MIN_DEGREE from the environment
+// (tuning; 0 MB turns the bitmaps off).
+static void hub_limits(size_t &bytes, int32_t &min_degree) {
+    bytes = kHubBitmapBytes;
+    min_degree = kHubMinDegree;
+    if (const char *s = std::getenv("GI_HUB_BITMAP_MB")) bytes = static_cast<size_t>(std::strtoull(s, nullptr, 10)) << 20;
+    if (const char *s = std::getenv("GI_HUB_MIN_DEGREE")) min_degree = std::max(1, std::atoi(s));
+}
+
 static int build_hubs(gi_graph *g, const int64_t *vertex, cudaStream_t st) {
+    size_t budget = 0;
+    int32_t min_degree = 0;
+    hub_limits(budget, min_degree);
     const int64_t words = (static_cast<int64_t>(g->v_cnt) + 31) / 32;
-    const int64_t max_hubs = static_cast<int64_t>(kHubBitmapBytes / (static_cast<size_t>(words) * sizeof(uint32_t)));
-    if (max_hubs < 1 || g->max_degree < kHubMinDegree) return GI_OK;
+    const int64_t max_hubs = static_cast<int64_t>(budget / (static_cast<size_t>(words) * sizeof(uint32_t)));
+    if (max_hubs < 1 || g->max_degree < min_degree) return GI_OK;
     std::vector<int32_t> big;
     for (int32_t v = 0; v < g->v_cnt; ++v) {
         const int64_t d = vertex[v + 1] - vertex[v];
-        if (d >= kHubMinDegree) big.push_back(static_cast<int32_t>(d));
+        if (d >= min_degree) big.push_back(static_cast<int32_t>(d));
     }
-    int32_t T = kHubMinDegree;
+    int32_t T = min_degree;
     if (static_cast<int64_t>(big.size()) > max_hubs) {
         std::nth_element(big.begin(), big.begin() + max_hubs, big.end(), std::greater<int32_t>());
         T = big[static_cast<size_t>(max_hubs)] + 1;  // the (max_hubs+1)-th largest degree is left out

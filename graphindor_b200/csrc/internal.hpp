@@ -67,6 +67,8 @@ struct DevPlan {
     int32_t stop;               // depth closed in form: n - iep_k with IEP, else n - 1
     int32_t leaf_depth;         // stop - 1 when its candidates run one per lane, else -1
     int32_t lane_budget;        // leaf candidates costlier than this for one lane go to the warp
+    int32_t leaf_flat;          // 1: leaf probes spread evenly over the warp's lanes (leaf_level_flat)
+    int32_t flat_first;         // 1: the DFS ends at depth 2 and a chunk's edges are counted as one flat leaf
     int32_t loop2_kind;         // bound of the depth-2 loop set: 0 d(v0), 1 d(v1), 2 min, -1 none
     int32_t pdepth[GI_MAX_PREFIX];  // last member (position) of each prefix
     int32_t father[GI_MAX_PREFIX];
@@ -89,6 +91,18 @@ struct DevPlan {
     int32_t iep_flag[GI_MAX_IEP_TERMS];
     int32_t iep_pos[GI_MAX_IEP_TERMS];
 };
+
+// The even-spread leaf (leaf_level_flat) numbers the probes of 32 candidates
+// with 32-bit ints: it is used only on graphs whose largest degree is below
+// this.
+constexpr int64_t kFlatLeafMaxDegree = int64_t(1) << 26;
+
+// The plan as a kernel receives it for a graph of the given largest degree.
+inline DevPlan plan_for_graph(const DevPlan &P, int64_t max_degree) {
+    DevPlan d = P;
+    if (max_degree >= kFlatLeafMaxDegree) d.leaf_flat = d.flat_first = 0;
+    return d;
+}
 
 }  // namespace gi
 

@@ -206,7 +206,7 @@ extern "C" int gi_count_noalloc(const int64_t *d_vertex, const int32_t *d_edge, 
     const int64_t stride = std::max<int64_t>(host.max_degree_vertices >= 2 ? host.max_degree : host.second_degree, 1);
 
     // As many warps as the scratch holds, at most the grid gi_count uses.
-    const DevPlan &P = p->dev;
+    const DevPlan P = plan_for_graph(p->dev, host.max_degree);
     const int64_t per_warp = static_cast<int64_t>(P.n_slots) * stride * static_cast<int64_t>(sizeof(uint32_t));
     const int64_t room = static_cast<int64_t>(kScratchBytes - kHeaderBytes);
     int blocks_per_sm = 1;
