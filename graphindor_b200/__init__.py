@@ -364,20 +364,24 @@ class LabeledGraph:
 
     @classmethod
     def from_csr(cls, vertex: np.ndarray, edge: np.ndarray, labels: np.ndarray,
-                 order: Optional[np.ndarray] = None) -> "LabeledGraph":
+                 order: Optional[np.ndarray] = None, device: bool = False, stream=None) -> "LabeledGraph":
         """``vertex``/``edge``: symmetric CSR in original ids; ``labels``:
         original label value per vertex; ``order``: the order of the vertex
-        lines (default ascending id)."""
+        lines (default ascending id).  ``device``: build the renumbered,
+        bucketed structure on the current GPU (gi_labeled_graph_create_device)
+        instead of on the host; the result is the same."""
         vertex = np.ascontiguousarray(vertex, dtype=np.int64)
         edge = np.ascontiguousarray(edge, dtype=np.int32)
         labels = np.ascontiguousarray(labels, dtype=np.uint32)
         if order is not None:
             order = np.ascontiguousarray(order, dtype=np.int32)
         h = C.c_void_p()
-        check(lib().gi_labeled_graph_create(len(vertex) - 1, vertex.ctypes.data,
-                                            edge.ctypes.data if edge.size else None, labels.ctypes.data,
-                                            order.ctypes.data if order is not None else None, C.byref(h)),
-              "gi_labeled_graph_create")
+        args = (len(vertex) - 1, vertex.ctypes.data, edge.ctypes.data if edge.size else None, labels.ctypes.data,
+                order.ctypes.data if order is not None else None)
+        if device:
+            check(lib().gi_labeled_graph_create_device(*args, stream, C.byref(h)), "gi_labeled_graph_create_device")
+        else:
+            check(lib().gi_labeled_graph_create(*args, C.byref(h)), "gi_labeled_graph_create")
         return cls(h)
 
     @classmethod

@@ -135,6 +135,8 @@ _SIGS = {
     "gi_motif_count": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.POINTER(Stats)]),
     "gi_labeled_graph_create": (C.c_int, [C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                           C.POINTER(C.c_void_p)]),
+    "gi_labeled_graph_create_device": (C.c_int, [C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                                 C.c_void_p, C.POINTER(C.c_void_p)]),
     "gi_labeled_graph_load_adj": (C.c_int, [C.c_char_p, C.POINTER(C.c_void_p)]),
     "gi_labeled_graph_destroy": (C.c_int, [C.c_void_p]),
     "gi_labeled_graph_get_info": (C.c_int, [C.c_void_p, C.POINTER(LabeledGraphInfo)]),

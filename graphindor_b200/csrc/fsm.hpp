@@ -28,6 +28,9 @@ struct gi_labeled_graph {
     uint32_t *d_edge = nullptr;
     uint32_t *d_bucket = nullptr;
     uint32_t *d_label_start = nullptr;
+    // Built on the device (labeled_ingest.cu): edge and bucket exist only
+    // there until an export downloads them.
+    bool device_built = false;
     std::mutex mu;  // serialises the FSM runs on one handle
 };
 
@@ -51,6 +54,10 @@ struct FsmRunStats {
     int64_t candidates = 0;
     int launches = 0;
 };
+
+// Host copies of the lists and buckets of a graph built on the device
+// (labeled_ingest.cu); nothing to do for a host-built graph.
+int labeled_graph_download(const gi_labeled_graph *g);
 
 // Copies the bucketed structure to the graph's device (fsm.cu).
 int fsm_upload(gi_labeled_graph *g);

@@ -492,6 +492,10 @@ int gi_labeled_graph_get_info(const gi_labeled_graph *g, gi_labeled_graph_info *
 int gi_labeled_graph_export(const gi_labeled_graph *g, int32_t *new_id, int32_t *v_label, uint32_t *label_value,
                             uint32_t *label_start, uint32_t *bucket, uint32_t *edge) {
     if (!g) return fail(GI_EINVAL, "NULL graph");
+    if (bucket || edge) {
+        const int st = labeled_graph_download(g);
+        if (st != GI_OK) return st;
+    }
     if (new_id) std::copy(g->new_id.begin(), g->new_id.end(), new_id);
     if (v_label) std::copy(g->v_label.begin(), g->v_label.end(), v_label);
     if (label_value) std::copy(g->label_value.begin(), g->label_value.end(), label_value);

@@ -354,6 +354,16 @@ int gi_mlp_train(const float *X, const float *y, int rows, int in, int hidden, i
  * list that is not symmetric.  The structure is copied to the current device. */
 int gi_labeled_graph_create(int32_t v_cnt, const int64_t *vertex, const int32_t *edge, const uint32_t *labels,
                             const int32_t *order, gi_labeled_graph **out);
+/* The same structure as gi_labeled_graph_create, built on the current device
+ * (GPU ingest; reference src/dataloader.cpp:440-620 does it on the host):
+ * degrees, the symmetry check, the renumbering by (label, -degree, id), the
+ * renamed and sorted neighbour lists and the label buckets are computed by
+ * kernels and device sorts; only the first-seen label pass and the sort of
+ * at most 255 (label, maximum degree) pairs run on the host.  The bucketed
+ * lists stay on the device (gi_labeled_graph_export downloads them).
+ * Additionally GI_EOVERFLOW for 2^31 or more neighbour entries. */
+int gi_labeled_graph_create_device(int32_t v_cnt, const int64_t *vertex, const int32_t *edge, const uint32_t *labels,
+                                   const int32_t *order, gi_stream stream, gi_labeled_graph **out);
 /* Parses a .adj text file: first token v_cnt, then one line per vertex
  * "id label nbr nbr ...". */
 int gi_labeled_graph_load_adj(const char *path, gi_labeled_graph **out);
