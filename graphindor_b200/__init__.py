@@ -18,7 +18,8 @@ from ._native import GIError, check, lib
 
 __all__ = ["Pattern", "Schedule_IEP", "Graph", "pattern_matching", "clique_count", "motif_counting",
            "motif_patterns", "GIError", "lib", "write_g", "read_g", "LabeledGraph", "fsm", "fsm_plan",
-           "FsmResult", "PATENTS_TRI_CNT", "YOUTUBE_TRI_CNT", "Batch", "load_cost_model"]
+           "FsmResult", "PATENTS_TRI_CNT", "YOUTUBE_TRI_CNT", "Batch", "load_cost_model", "autotune",
+           "autotune_clear"]
 
 
 class Pattern:
@@ -128,6 +129,20 @@ class Schedule_IEP:
             out[key] = list(buf[: n_raw.value])
         return out
 
+    @property
+    def variant(self) -> dict:
+        """The plan's kernel variant (speed only, never counts)."""
+        v = N.Variant()
+        check(lib().gi_plan_get_variant(self._h, C.byref(v)), "gi_plan_get_variant")
+        return {"leaf_flat": v.leaf_flat, "lane_budget": v.lane_budget, "occupancy": v.occupancy}
+
+    @variant.setter
+    def variant(self, v: dict) -> None:
+        cur = self.variant
+        cur.update(v)
+        check(lib().gi_plan_set_variant(self._h, C.byref(N.Variant(cur["leaf_flat"], cur["lane_budget"],
+                                                                    cur["occupancy"]))), "gi_plan_set_variant")
+
     @classmethod
     def learned(cls, pattern: Pattern, graph: "Graph", enable_iep: bool = True,
                 model_path: Optional[str] = None) -> "Schedule_IEP":
@@ -172,6 +187,25 @@ class Schedule_IEP:
             r = [(rs[(i * N.GI_MAX_PREFIX + j) * 2], rs[(i * N.GI_MAX_PREFIX + j) * 2 + 1]) for j in range(nr[i])]
             out.append((list(orders[i * n:(i + 1) * n]), r, costs[i], divs[i]))
         return out
+
+
+def autotune(graph: "Graph", schedule: Schedule_IEP, *, sample_edges: int = 0, max_ms: float = 0.0, reps: int = 0,
+             use_cache: bool = True, stream: int = 0) -> dict:
+    """Times the kernel variants of `schedule` on a sample of `graph` and
+    keeps the fastest in the plan (gi_autotune); the choice is cached for the
+    class of (plan, graph), and batches apply cached choices to their jobs."""
+    o = N.TuneOptions(int(sample_edges), float(max_ms), int(reps), int(use_cache))
+    info = N.TuneInfo()
+    check(lib().gi_autotune(graph.handle, schedule.handle, C.c_void_p(stream) if stream else None, C.byref(o),
+                            C.byref(info)), "gi_autotune")
+    c = info.chosen
+    return {"chosen": {"leaf_flat": c.leaf_flat, "lane_budget": c.lane_budget, "occupancy": c.occupancy},
+            "cached": bool(info.cached), "candidates": info.candidates, "best_ms": info.best_ms,
+            "default_ms": info.default_ms, "sample_edges": info.sample_edges}
+
+
+def autotune_clear() -> None:
+    check(lib().gi_autotune_clear(), "gi_autotune_clear")
 
 
 COST_MODEL_PATH = __import__("pathlib").Path(__file__).resolve().parent / "schedule_cost" / "weights.bin"

@@ -78,6 +78,19 @@ class Stats(C.Structure):
                 ("edge_offset", C.c_int64)]
 
 
+class Variant(C.Structure):
+    _fields_ = [("leaf_flat", C.c_int32), ("lane_budget", C.c_int32), ("occupancy", C.c_int32)]
+
+
+class TuneOptions(C.Structure):
+    _fields_ = [("sample_edges", C.c_int64), ("max_ms", C.c_double), ("reps", C.c_int32), ("use_cache", C.c_int32)]
+
+
+class TuneInfo(C.Structure):
+    _fields_ = [("chosen", Variant), ("cached", C.c_int32), ("candidates", C.c_int32), ("best_ms", C.c_double),
+                ("default_ms", C.c_double), ("sample_edges", C.c_int64)]
+
+
 class LabeledGraphInfo(C.Structure):
     _fields_ = [("v_cnt", C.c_int32), ("e_cnt", C.c_int64), ("l_cnt", C.c_int32), ("device", C.c_int32)]
 
@@ -138,6 +151,10 @@ _SIGS = {
     "gi_labeled_graph_create_device": (C.c_int, [C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                                  C.c_void_p, C.POINTER(C.c_void_p)]),
     "gi_labeled_graph_load_adj": (C.c_int, [C.c_char_p, C.POINTER(C.c_void_p)]),
+    "gi_plan_get_variant": (C.c_int, [C.c_void_p, C.POINTER(Variant)]),
+    "gi_plan_set_variant": (C.c_int, [C.c_void_p, C.POINTER(Variant)]),
+    "gi_autotune": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(TuneOptions), C.POINTER(TuneInfo)]),
+    "gi_autotune_clear": (C.c_int, []),
     "gi_labeled_graph_destroy": (C.c_int, [C.c_void_p]),
     "gi_labeled_graph_get_info": (C.c_int, [C.c_void_p, C.POINTER(LabeledGraphInfo)]),
     "gi_labeled_graph_export": (C.c_int, [C.c_void_p] + [C.c_void_p] * 6),

@@ -239,7 +239,10 @@ int gi_batch_create(gi_graph *const *graphs, const gi_plan *const *plans, int n_
         b->graphs.push_back(g);
         b->plans.push_back(p);
         b->divisor.push_back(static_cast<uint64_t>(p->sched->get_count_divisor()));
-        hplans.push_back(plan_for_graph(p->dev, g->max_degree));
+        // The autotuner's cached variant for this job's class, if any.
+        DevPlan dp = p->dev;
+        tuned_plan(g, p->dev, dp);
+        hplans.push_back(plan_for_graph(dp, g->max_degree));
         const int64_t nch = (g->e_cnt + kTaskChunk - 1) / kTaskChunk;
         b->chunks.push_back(static_cast<unsigned long long>(nch));
         hjobs[j] = BatchJob{g->d_vertex, reinterpret_cast<const uint32_t *>(g->d_edge), g->d_edge_from, g->e_cnt,

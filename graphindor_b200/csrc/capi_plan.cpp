@@ -114,7 +114,9 @@ static int build_dev_plan(const Schedule_IEP &s, DevPlan &d) {
     if (const char *e = std::getenv("GI_LEAF_FLAT")) d.leaf_flat = std::atoi(e) != 0;
     // A DFS that ends at depth 2 (triangle- and diamond-like plans): the
     // first-level edges of a chunk are themselves the flat leaf's candidates.
-    d.flat_first = d.leaf_flat && d.stop == 2 && !(d.vertex_induced && anti_edge);
+    d.flat_first_ok = d.stop == 2 && !(d.vertex_induced && anti_edge);
+    d.flat_first = d.leaf_flat && d.flat_first_ok;
+    d.occupancy = 0;
     for (int p = 0; p < GI_MAX_PREFIX; ++p) d.pdepth[p] = p < tp ? s.get_prefix_data(p).back() : -1;
     // Splitting of the depth-2 loop: its set's members are a subset of {0, 1}.
     d.loop2_kind = -1;

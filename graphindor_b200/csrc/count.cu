@@ -288,9 +288,9 @@ static int build_split(gi_graph *g, const DevPlan &P, cudaStream_t st, int split
 using DfsKernel = decltype(&dfs_count_kernel<false, 1>);
 
 // The instantiation for a plan: byte counting on or off, and the occupancy
-// target by pattern size.
-DfsKernel pick_dfs_kernel(bool bytes_on, int n) {
-    const bool deep = n >= 6;
+// target (the plan's variant, else by pattern size).
+DfsKernel pick_dfs_kernel(bool bytes_on, const DevPlan &P) {
+    const bool deep = P.occupancy ? P.occupancy >= 16 : P.n >= 6;
     if (bytes_on) return deep ? dfs_count_kernel<true, 16> : dfs_count_kernel<true, 1>;
     return deep ? dfs_count_kernel<false, 16> : dfs_count_kernel<false, 1>;
 }
@@ -309,7 +309,7 @@ int count_impl(gi_graph *g, const DevPlan &plan, cudaStream_t st, uint64_t *raw_
     const int64_t edge_offset = edge_step > 1 ? stats->edge_offset : 0;
     if (edge_offset < 0 || edge_offset >= edge_step) return fail(GI_EINVAL, "edge_offset outside [0, edge_step)");
     cudaError_t e;
-    const auto kernel = pick_dfs_kernel(bytes_on, P.n);
+    const auto kernel = pick_dfs_kernel(bytes_on, P);
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, kernel, kBlockThreads, 0);
     if (e != cudaSuccess) return cuda_fail(e, "occupancy query");
     const int blocks = sms * std::max(1, blocks_per_sm);

@@ -69,6 +69,8 @@ struct DevPlan {
     int32_t lane_budget;        // leaf candidates costlier than this for one lane go to the warp
     int32_t leaf_flat;          // 1: leaf probes spread evenly over the warp's lanes (leaf_level_flat)
     int32_t flat_first;         // 1: the DFS ends at depth 2 and a chunk's edges are counted as one flat leaf
+    int32_t flat_first_ok;      // the plan allows flat_first (set with leaf_flat)
+    int32_t occupancy;          // resident blocks per SM the kernel is built for: 0 by pattern size, 1 or 16
     int32_t loop2_kind;         // bound of the depth-2 loop set: 0 d(v0), 1 d(v1), 2 min, -1 none
     int32_t pdepth[GI_MAX_PREFIX];  // last member (position) of each prefix
     int32_t father[GI_MAX_PREFIX];
@@ -103,6 +105,12 @@ inline DevPlan plan_for_graph(const DevPlan &P, int64_t max_degree) {
     if (max_degree >= kFlatLeafMaxDegree) d.leaf_flat = d.flat_first = 0;
     return d;
 }
+
+// Kernel variants (autotune.cpp): set a variant's fields in a plan, and the
+// plan with the cached tuned variant of its class on graph g (false when
+// none is cached).
+void variant_apply(DevPlan &P, const gi_variant &v);
+bool tuned_plan(const gi_graph *g, const DevPlan &P, DevPlan &out);
 
 }  // namespace gi
 

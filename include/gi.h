@@ -236,6 +236,45 @@ int gi_count(const gi_graph *g, const gi_plan *p, gi_stream stream, uint64_t *ou
 int gi_count_shard(const gi_graph *g, const gi_plan *p, int32_t shard, int32_t num_shards, gi_stream stream,
                    uint64_t *raw_sum, gi_stats *stats);
 
+/* -------------------------------------------------------------- autotuner */
+
+/* Kernel variant of a plan: changes the counting kernel's speed, never its
+ * counts.  The reference has one configuration, fixed at compile time
+ * (reference gpu/function/pattern_matching.cuh:7-9, gpu/gpu_graph.cu:33). */
+typedef struct gi_variant {
+    int32_t leaf_flat;   /* 1: leaf probes spread evenly over a warp's lanes; 0: a candidate per lane */
+    int32_t lane_budget; /* leaf_flat 0: candidates costlier than this run on the whole warp (0 = keep) */
+    int32_t occupancy;   /* resident blocks per SM the kernel is built for: 1, 16, or 0 = by pattern size */
+} gi_variant;
+int gi_plan_get_variant(const gi_plan *p, gi_variant *out);
+int gi_plan_set_variant(gi_plan *p, const gi_variant *v);
+
+typedef struct gi_tune_options {
+    int64_t sample_edges; /* first-level edges in the timed sample (0 = 16384) */
+    double max_ms;        /* a variant slower than this on the sample is dropped (0 = 250) */
+    int32_t reps;         /* timed runs per variant, the fastest kept (0 = 2) */
+    int32_t use_cache;    /* 1: reuse a choice cached for the same class of plan and graph */
+} gi_tune_options;
+
+typedef struct gi_tune_info {
+    gi_variant chosen;
+    int32_t cached;       /* 1: taken from the cache, nothing timed */
+    int32_t candidates;   /* variants timed */
+    double best_ms;       /* the chosen variant's time on the sample */
+    double default_ms;    /* the plan's own variant's time on the sample */
+    int64_t sample_edges; /* first-level edges timed */
+} gi_tune_info;
+
+/* Times every variant (leaf spread or per lane with lane budgets 256 and
+ * 2048, each at occupancy 1 and 16) on an edge subset of g (each task
+ * whole; every variant must give the same raw sum, else GI_ECUDA), sets
+ * the fastest in p and caches it for the class of (p, g): pattern size, IEP
+ * depth, depth-2 split, first-level restriction, log2 of the edge count and
+ * of the largest degree.  gi_batch_create applies cached choices to its
+ * jobs.  opt and info may be NULL. */
+int gi_autotune(const gi_graph *g, gi_plan *p, gi_stream stream, const gi_tune_options *opt, gi_tune_info *info);
+int gi_autotune_clear(void);
+
 /* No counterpart in the reference.  The count of gi_count for callers that
  * must not allocate device memory when they ask for it: code whose GPU
  * memory is owned by another framework's pool, a serving loop that cannot

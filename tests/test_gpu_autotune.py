@@ -1,0 +1,69 @@
+"""The autotuner (gi_autotune) and kernel variants on the GPU: every
+variant of a plan counts exactly what the default does (the raw sums are
+integers and must be identical), the tuner keeps one of the variants it
+timed and caches it per class of (plan, graph), and a batch built after
+tuning applies the cached variants and still counts what single counts do."""
+from __future__ import annotations
+
+import pytest
+
+import graphindor_b200 as gi
+from graphindor_b200 import gen
+
+pytestmark = pytest.mark.gpu
+
+PATTERNS = [(4, "0111101111001100"), (4, "0110100110010110"), (5, "0101110101010101010011000"),
+            (5, "0111110111110111110111110"), (6, "011100101010110001100011010101001110"), (3, "011101110")]
+
+
+def test_every_variant_counts_the_same():
+    g = gen.rmat(12, 12.0, 31)
+    dg = gi.Graph.from_csr(g.vertex, g.edge)
+    for n, adj in PATTERNS:
+        s = gi.Schedule_IEP(gi.Pattern(n, adj), g.v_cnt, g.e_cnt, 0)
+        want = gi.pattern_matching(dg, s).raw_sum
+        for flat in (0, 1):
+            for budget in (64, 256, 2048):
+                for occ in (0, 1, 16):
+                    s.variant = {"leaf_flat": flat, "lane_budget": budget, "occupancy": occ}
+                    assert gi.pattern_matching(dg, s).raw_sum == want, (adj, flat, budget, occ)
+        # Edge subsets too (the tuner's sample).
+        s.variant = {"leaf_flat": 1, "occupancy": 16}
+        tot = sum(gi.count_edges(dg, s, 5, off).raw_sum for off in range(5)) % (1 << 64)
+        assert tot == want
+
+
+def test_tuner_picks_a_timed_variant_and_caches_it():
+    gi.autotune_clear()
+    g = gen.rmat(13, 10.0, 32)
+    dg = gi.Graph.from_csr(g.vertex, g.edge)
+    for n, adj in PATTERNS[:4]:
+        s = gi.Schedule_IEP(gi.Pattern(n, adj), g.v_cnt, g.e_cnt, 0)
+        want = gi.pattern_matching(dg, s).raw_sum
+        info = gi.autotune(dg, s, sample_edges=4096)
+        assert not info["cached"] and info["candidates"] == 6
+        assert info["best_ms"] > 0 and info["best_ms"] <= info["default_ms"] + 1e-9
+        assert s.variant["leaf_flat"] == info["chosen"]["leaf_flat"]
+        assert s.variant["occupancy"] == info["chosen"]["occupancy"]
+        assert gi.pattern_matching(dg, s).raw_sum == want
+        s2 = gi.Schedule_IEP(gi.Pattern(n, adj), g.v_cnt, g.e_cnt, 0)
+        again = gi.autotune(dg, s2)
+        assert again["cached"] and again["chosen"] == info["chosen"]
+
+
+def test_batch_applies_tuned_variants():
+    gi.autotune_clear()
+    graphs = [gen.rmat(11, 8.0, 40), gen.rmat(12, 14.0, 41)]
+    dgs = [gi.Graph.from_csr(g.vertex, g.edge) for g in graphs]
+    jobs, want = [], []
+    for dg, g in zip(dgs, graphs):
+        for n, adj in PATTERNS:
+            s = gi.Schedule_IEP(gi.Pattern(n, adj), g.v_cnt, g.e_cnt, 0)
+            want.append(gi.pattern_matching(dg, s).count)
+            gi.autotune(dg, s, sample_edges=2048)
+            jobs.append((dg, s))
+    b = gi.Batch(jobs)
+    for _ in range(2):  # capture, then replay
+        counts, lat, _ = b.run()
+        assert counts == want
+        assert all(x >= 0 for x in lat)
