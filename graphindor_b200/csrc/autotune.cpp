@@ -125,7 +125,27 @@ int gi_autotune(const gi_graph *g, gi_plan *p, gi_stream stream, const gi_tune_o
         }
     }
     const DevPlan original = p->dev;
-    const int64_t step = std::max<int64_t>(1, g->e_cnt / std::max<int64_t>(1, o.sample_edges));
+    // Calibrate the sample with the plan's own variant: fewer edges while it
+    // runs past max_ms, more while it takes under a fiftieth of it.
+    int64_t step = std::max<int64_t>(1, g->e_cnt / std::max<int64_t>(1, o.sample_edges));
+    for (int round = 0; round < 12; ++round) {
+        gi_stats s{};
+        s.edge_step = step;
+        s.budget_ms = o.max_ms;
+        uint64_t raw = 0;
+        const int rc = gi_count_shard(g, p, 0, 1, stream, &raw, &s);
+        if (rc == GI_ETIMEOUT) {
+            if (step >= g->e_cnt) break;  // a single edge is already too slow
+            step = std::min<int64_t>(std::max<int64_t>(g->e_cnt, 1), step * 8);
+            continue;
+        }
+        if (rc != GI_OK) return rc;
+        if (s.kernel_ms + s.prep_ms < o.max_ms / 50 && step > 1) {
+            step = std::max<int64_t>(1, step / 4);
+            continue;
+        }
+        break;
+    }
     const int budgets[2] = {256, 2048};
     std::vector<gi_variant> cands;
     for (int occ : {1, 16}) {

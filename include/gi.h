@@ -267,7 +267,9 @@ typedef struct gi_tune_info {
 
 /* Times every variant (leaf spread or per lane with lane budgets 256 and
  * 2048, each at occupancy 1 and 16) on an edge subset of g (each task
- * whole; every variant must give the same raw sum, else GI_ECUDA), sets
+ * whole; every variant must give the same raw sum, else GI_ECUDA; the
+ * subset is first resized until the plan's own variant takes between a
+ * fiftieth of max_ms and max_ms, starting from sample_edges edges), sets
  * the fastest in p and caches it for the class of (p, g): pattern size, IEP
  * depth, depth-2 split, first-level restriction, log2 of the edge count and
  * of the largest degree.  gi_batch_create applies cached choices to its
