@@ -22,7 +22,7 @@ GI_OK, GI_EINVAL, GI_ENOMEM, GI_ECUDA, GI_ETIMEOUT, GI_EOVERFLOW, GI_EIO, GI_ENO
 class GraphInfo(C.Structure):
     _fields_ = [("v_cnt", C.c_int32), ("e_cnt", C.c_int64), ("tri_cnt", C.c_int64),
                 ("max_degree", C.c_int32), ("max_intersection_size", C.c_int32), ("n_hubs", C.c_int32),
-                ("hub_min_degree", C.c_int32)]
+                ("hub_min_degree", C.c_int32), ("hash_min_degree", C.c_int32), ("hash_slots", C.c_int64)]
 
 
 class PlanDesc(C.Structure):

@@ -36,6 +36,7 @@ struct BatchJob {
     int32_t plan;         // index into the batch's plans
     uint32_t v_cnt;
     HubIndex hubs;        // the graph's hub bitmaps
+    HashIndex hashes;     // and adjacency hash sets
 };
 
 // Counter slots of a batch: [0] chunk cursor, [1] launch start (min over
@@ -112,6 +113,7 @@ __global__ void __launch_bounds__(kBlockThreads)
         enter_job(plans, J, job, cur, P, lane);
         Ctx<false> ctx{P, J.vertex, J.edge, slots, slot_stride, w, lane, 0ull};
         ctx.hubs = J.hubs;
+        ctx.hashes = J.hashes;
         ctx.hq = hq;
         ctx.hq.job = job;
         ctx.hq.v_cnt = J.v_cnt;
@@ -161,6 +163,7 @@ __global__ void __launch_bounds__(kBlockThreads)
             enter_job(plans, J, job, cur, P, lane);
             Ctx<false> ctx{P, J.vertex, J.edge, slots, slot_stride, w, lane, 0ull};
             ctx.hubs = J.hubs;
+            ctx.hashes = J.hashes;
             ctx.hq = hq;
             ctx.hq.job = job;
             ctx.hq.v_cnt = J.v_cnt;
@@ -246,7 +249,7 @@ int gi_batch_create(gi_graph *const *graphs, const gi_plan *const *plans, int n_
         const int64_t nch = (g->e_cnt + kTaskChunk - 1) / kTaskChunk;
         b->chunks.push_back(static_cast<unsigned long long>(nch));
         hjobs[j] = BatchJob{g->d_vertex, reinterpret_cast<const uint32_t *>(g->d_edge), g->d_edge_from, g->e_cnt,
-                            chunk, j, static_cast<uint32_t>(g->v_cnt), hubs_of(g)};
+                            chunk, j, static_cast<uint32_t>(g->v_cnt), hubs_of(g), hashes_of(g)};
         chunk += nch;
         b->slot_stride = std::max<int64_t>(b->slot_stride, g->max_isect);
         b->slots_per_warp = std::max<int64_t>(b->slots_per_warp, p->dev.n_slots);

@@ -81,7 +81,7 @@ __global__ void __launch_bounds__(kBlockThreads, kMinBlocks)
                      int64_t num_shards, int64_t n_chunks, int64_t perm_a, int64_t perm_b,
                      unsigned long long hard_ns, unsigned long long max_claims, Handoff *hitems,
                      unsigned long long hcap, uint32_t hepoch, uint32_t v_cnt, int64_t edge_step,
-                     int64_t edge_offset, HubIndex hubs) {
+                     int64_t edge_offset, HubIndex hubs, HashIndex hashes) {
     __shared__ WarpState states[kWarpsPerBlock];
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
@@ -94,6 +94,7 @@ __global__ void __launch_bounds__(kBlockThreads, kMinBlocks)
     c.t_start = t_start;
     c.hard_ns = hard_ns;
     c.hubs = hubs;
+    c.hashes = hashes;
     if (hitems) {
         c.hq.items = hitems;
         c.hq.cap = hcap;
@@ -387,7 +388,7 @@ int count_impl(gi_graph *g, const DevPlan &plan, cudaStream_t st, uint64_t *raw_
                                              shard, num_shards, n_chunks, perm_a, perm_b, hard_ns, max_claims,
                                              hitems, kHandoffCap, g->handoff_epoch,
                                              static_cast<uint32_t>(g->v_cnt), edge_step, edge_offset,
-                                             hubs_of(g));
+                                             hubs_of(g), hashes_of(g));
     launches += 1;
     e = cudaGetLastError();
     cudaEventRecord(t1, st);

@@ -29,6 +29,7 @@ struct WarpState {
     const uint32_t *set_ptr[GI_MAX_PREFIX];
     int32_t set_size[GI_MAX_PREFIX];
     int32_t hub[GI_MAX_PREFIX];        // row in the graph's hub bitmaps when the set is a hub's list, else -1
+    int32_t src[GI_MAX_PREFIX];        // v when the set is N(v) itself (an alias), else -1
     uint32_t emb_mask[GI_MAX_PREFIX];  // leaf level: which emb[0, D) lie in each earlier set
     uint32_t emb[GI_MAX_PATTERN + 1];
     int32_t cursor[GI_MAX_PATTERN + 1];
@@ -76,6 +77,45 @@ inline HubIndex hubs_of(const gi_graph *g) {
 
 __device__ __forceinline__ bool hub_test(const HubIndex &H, int r, uint32_t x) {
     return (__ldg(&H.bits[static_cast<int64_t>(r) * H.words + (x >> 5)]) >> (x & 31)) & 1u;
+}
+
+// Adjacency hash sets (graph.cu): vertex v of degree >= min_degree has the
+// table slots[off[v] .. off[v+1]) of a power-of-two size, holding N(v) by
+// linear probing from the multiplicative hash; empty slots are 0xffffffff.
+struct HashIndex {
+    const uint32_t *slots = nullptr;
+    const int64_t *off = nullptr;
+    int32_t min_degree = 0x7fffffff;
+};
+
+inline HashIndex hashes_of(const gi_graph *g) {
+    HashIndex h;
+    if (g->hash_slots > 0) {
+        h.slots = g->d_hash;
+        h.off = g->d_hash_off;
+        h.min_degree = g->hash_min_degree;
+    }
+    return h;
+}
+
+// v's table and log2 of its size, or nullptr when v (degree deg) has none.
+__device__ __forceinline__ const uint32_t *hash_table(const HashIndex &H, uint32_t v, int deg, int &bits) {
+    if (deg < H.min_degree) return nullptr;
+    const int64_t a = __ldg(&H.off[v]), b = __ldg(&H.off[v + 1]);
+    bits = __ffsll(b - a) - 1;
+    return H.slots + a;
+}
+
+__device__ __forceinline__ bool hash_contains(const uint32_t *t, int bits, uint32_t x) {
+    const uint32_t mask = (1u << bits) - 1u;
+    uint32_t s = (x * 2654435769u) >> (32 - bits);
+    for (uint32_t k = 0; k <= mask; ++k) {
+        const uint32_t y = __ldg(&t[s]);
+        if (y == x) return true;
+        if (y == 0xffffffffu) return false;
+        s = (s + 1) & mask;
+    }
+    return false;
 }
 
 // Row of v's bitmap, or -1 when v (degree deg) is not a hub.
@@ -440,43 +480,54 @@ __device__ __forceinline__ unsigned long long iep_combine(const DevPlan &P, cons
     return acc;
 }
 
+// One sorted list of a pair, with the structures that answer membership
+// in it: a hub's bitmap row (hub >= 0) or an adjacency hash set (hash).
+struct ListRef {
+    const uint32_t *p;
+    int n;
+    int hub;
+    const uint32_t *hash;
+    int hash_bits;
+};
+
+// Steps to test one element for membership in l: one bitmap load, about two
+// hash-set loads, or a binary search.
+__device__ __forceinline__ int member_cost(const ListRef &l) {
+    return l.hub >= 0 ? 1 : l.hash ? 2 : 33 - __clz(l.n + 1);
+}
+
 // Per lane: |a ∩ b| and |a ∩ b ∩ [0, bound)| for the lane's own pair of
 // sorted lists, with the work of all 32 pairs spread evenly over the lanes.
 // Each lane's probes are the elements of one list of its pair, tested for
-// membership in the other: through a hub's bitmap row when either list is a
-// hub's (ha / hb >= 0; one load per probe), else by binary search of the
-// smaller list's elements in the larger one.  The warp walks the
-// concatenation of all lanes' probes 32 at a time: a lane finds the pair
-// owning its probe (binary search over the exclusive scan of the probe
-// counts), tests it, and the hit ballots are split back to the owners by
-// their probe ranges.  Every lane does one test per step whatever the list
-// sizes, and consecutive lanes read consecutive elements of a list.  Without
-// need_total only elements below bound are probed (tot == bel).  A lane with
-// active false has no probes and gets 0.  All lanes must call it together.
-__device__ __forceinline__ void flat_count(const HubIndex &H, const uint32_t *a, int na, int ha, const uint32_t *b,
-                                           int nb, int hb, uint32_t bound, bool need_total, bool active, int lane,
-                                           int &tot, int &bel) {
-    const uint32_t *probe = a, *tgt = b;
-    int n = 0, tn = -1;  // tn < 0: tgt is a bitmap row
+// membership in the other through the other's bitmap row, hash set or, for a
+// plain list, binary search; the direction with fewer expected steps is
+// taken.  The warp walks the concatenation of all lanes' probes 32 at a
+// time: a lane finds the pair owning its probe (binary search over the
+// exclusive scan of the probe counts), tests it, and the hit ballots are
+// split back to the owners by their probe ranges.  Every lane does one test
+// per step whatever the list sizes, and consecutive lanes read consecutive
+// elements of a list.  Without need_total only elements below bound are
+// probed (tot == bel).  A lane with active false has no probes and gets 0.
+// All lanes must call it together.
+__device__ __forceinline__ void flat_count(const HubIndex &H, const ListRef &a, const ListRef &b, uint32_t bound,
+                                           bool need_total, bool active, int lane, int &tot, int &bel) {
+    const uint32_t *probe = a.p, *tgt = b.p;
+    int n = 0, code = 0;  // code >= 0: binary search in tgt[0, code); -1: bitmap row; <= -2: hash of -2 - code bits
     if (active) {
-        if (ha >= 0 && na >= nb) {
-            probe = b;
-            n = nb;
-            tgt = H.bits + static_cast<int64_t>(ha) * H.words;
-        } else if (hb >= 0) {
-            probe = a;
-            n = na;
-            tgt = H.bits + static_cast<int64_t>(hb) * H.words;
-        } else if (na <= nb) {
-            probe = a;
-            n = na;
-            tgt = b;
-            tn = nb;
+        const bool a_in_b = static_cast<int64_t>(a.n) * member_cost(b) <= static_cast<int64_t>(b.n) * member_cost(a);
+        const ListRef &pr = a_in_b ? a : b;
+        const ListRef &tg = a_in_b ? b : a;
+        probe = pr.p;
+        n = pr.n;
+        if (tg.hub >= 0) {
+            tgt = H.bits + static_cast<int64_t>(tg.hub) * H.words;
+            code = -1;
+        } else if (tg.hash) {
+            tgt = tg.hash;
+            code = -2 - tg.hash_bits;
         } else {
-            probe = b;
-            n = nb;
-            tgt = a;
-            tn = na;
+            tgt = tg.p;
+            code = tg.n;
         }
         if (!need_total) n = lower_bound_u32(probe, n, bound);
     }
@@ -501,12 +552,17 @@ __device__ __forceinline__ void flat_count(const HubIndex &H, const uint32_t *a,
         const int k = item - __shfl_sync(kFull, off, c);
         const uint32_t *pc = reinterpret_cast<const uint32_t *>(__shfl_sync(kFull, pa, c));
         const uint32_t *tc = reinterpret_cast<const uint32_t *>(__shfl_sync(kFull, ta, c));
-        const int tnc = __shfl_sync(kFull, tn, c);
+        const int cc = __shfl_sync(kFull, code, c);
         const uint32_t bc = __shfl_sync(kFull, bound, c);
         bool hit = false, below = false;
         if (item < total) {
             const uint32_t x = pc[k];
-            hit = tnc < 0 ? ((__ldg(&tc[x >> 5]) >> (x & 31)) & 1u) != 0 : contains_u32(tc, tnc, x);
+            if (cc >= 0)
+                hit = contains_u32(tc, cc, x);
+            else if (cc == -1)
+                hit = ((__ldg(&tc[x >> 5]) >> (x & 31)) & 1u) != 0;
+            else
+                hit = hash_contains(tc, -2 - cc, x);
             below = hit && x < bc;
         }
         const unsigned hm = __ballot_sync(kFull, hit), bm = __ballot_sync(kFull, below);
@@ -536,6 +592,7 @@ struct Ctx {
     bool aborted = false;
     HandoffQueue hq{};
     HubIndex hubs{};
+    HashIndex hashes{};
 
     // Offers [lo, hi) of depth d's loop to an idle warp (warp-uniform);
     // true when it was queued and is no longer this warp's to do.
@@ -586,6 +643,7 @@ struct Ctx {
                 if (lane == 0) {
                     w.set_ptr[p] = nb;
                     w.hub[p] = hv;
+                    w.src[p] = static_cast<int32_t>(v);
                 }
                 size = deg;
                 if (kBytesOn && account && lane == 0) bytes += 16;
@@ -607,6 +665,7 @@ struct Ctx {
                 if (lane == 0) {
                     if (out) w.set_ptr[p] = out;
                     w.hub[p] = -1;
+                    w.src[p] = -1;
                 }
                 if (kBytesOn && account && lane == 0) bytes += 4ull * (fn + deg + (out ? size : 0));
             }
@@ -875,20 +934,28 @@ struct Ctx {
         const int L = P.loop_set[stop];
         const bool last_level = P.iep_k == 0;
         int64_t l = 0;
-        int dv = 0, hv = -1;
+        int dv = 0, hv = -1, hv_bits = 0;
+        const uint32_t *hv_hash = nullptr;
         uint32_t bound = 0xffffffffu, mask_nv = 0;
         if (alive) {
             l = __ldg(&vertex[v]);
             dv = static_cast<int>(__ldg(&vertex[v + 1]) - l);
             hv = hub_row_of(hubs, v, dv);
+            hv_hash = hash_table(hashes, v, dv, hv_bits);
             if (last_level)
                 for (int r = P.restrict_last[stop]; r != -1; r = P.restrict_next[r]) {
                     const int idx = P.restrict_index[r];
                     bound = min(bound, idx == D ? v : early.emb(idx));
                 }
-            for (int u = 0; u < D; ++u) {
-                const uint32_t x = early.emb(u);
-                mask_nv |= static_cast<uint32_t>(hv >= 0 ? hub_test(hubs, hv, x) : contains_u32(edge + l, dv, x)) << u;
+            if (Early::kFirstEdge) {
+                mask_nv = 1u;  // v = v1 and emb[0] = v0 are the ends of an edge
+            } else {
+                for (int u = 0; u < D; ++u) {
+                    const uint32_t x = early.emb(u);
+                    const bool in = hv >= 0 ? hub_test(hubs, hv, x)
+                                            : hv_hash ? hash_contains(hv_hash, hv_bits, x) : contains_u32(edge + l, dv, x);
+                    mask_nv |= static_cast<uint32_t>(in) << u;
+                }
             }
         }
         const uint32_t *nv = edge + l;
@@ -912,8 +979,11 @@ struct Ctx {
             const uint32_t *fs = early.set_ptr(f);
             const int fn = early.set_size(f);
             const bool need_total = kBytesOn || !(last_level && p == L);
+            ListRef fa{fs, fn, early.hub(f), nullptr, 0};
+            const int fsrc = early.src(f);
+            if (fsrc >= 0) fa.hash = hash_table(hashes, static_cast<uint32_t>(fsrc), fn, fa.hash_bits);
             int tot, bel;
-            flat_count(hubs, fs, fn, early.hub(f), nv, dv, hv, bound, need_total, alive, lane, tot, bel);
+            flat_count(hubs, fa, ListRef{nv, dv, hv, hv_hash, hv_bits}, bound, need_total, alive, lane, tot, bel);
             size[p] = tot;
             if (p == L) below_L = bel;
             mask[p] = early.emb_mask(f) & mask_nv;
@@ -976,11 +1046,13 @@ struct Ctx {
 
     // The sets built before the leaf-parent depth, shared by the warp.
     struct EarlyShared {
+        static constexpr bool kFirstEdge = false;
         const WarpState &w;
         __device__ __forceinline__ uint32_t emb(int u) const { return w.emb[u]; }
         __device__ __forceinline__ const uint32_t *set_ptr(int q) const { return w.set_ptr[q]; }
         __device__ __forceinline__ int set_size(int q) const { return w.set_size[q]; }
         __device__ __forceinline__ int hub(int q) const { return w.hub[q]; }
+        __device__ __forceinline__ int src(int q) const { return w.src[q]; }
         __device__ __forceinline__ uint32_t emb_mask(int q) const { return w.emb_mask[q]; }
     };
 
@@ -1024,6 +1096,7 @@ struct Ctx {
     // The sets of depth 0 for a lane's own first-level edge (v0, v1): every
     // depth-0 prefix is N(v0), which holds v1 and not v0.
     struct EarlyEdge {
+        static constexpr bool kFirstEdge = true;
         uint32_t v0;
         const uint32_t *n0;
         int d0, h0;
@@ -1031,6 +1104,7 @@ struct Ctx {
         __device__ __forceinline__ const uint32_t *set_ptr(int) const { return n0; }
         __device__ __forceinline__ int set_size(int) const { return d0; }
         __device__ __forceinline__ int hub(int) const { return h0; }
+        __device__ __forceinline__ int src(int) const { return static_cast<int>(v0); }
         __device__ __forceinline__ uint32_t emb_mask(int) const { return 0u; }
     };
 

@@ -141,6 +141,106 @@ static int build_hubs(gi_graph *g, const int64_t *vertex, cudaStream_t st) {
     return GI_OK;
 }
 
+// Per-vertex hash sets of adjacency lists: a membership test against N(v) in
+// one or two loads instead of a binary search of log2 d(v) dependent loads.
+// Every vertex of degree >= T gets a table of next_pow2(2 d(v)) slots (load
+// at most 1/2, linear probing); T is the smallest value >= kHashMinDegree
+// for which all tables fit the budget (GI_HASH_MB, default kHashBytes; 0
+// turns them off; GI_HASH_MIN_DEGREE overrides kHashMinDegree).
+constexpr size_t kHashBytes = size_t(4) << 30;
+constexpr int32_t kHashMinDegree = 32;
+
+int64_t hash_capacity(int64_t deg) {
+    int64_t c = 2;
+    while (c < 2 * deg) c <<= 1;
+    return c;
+}
+
+namespace {
+// A warp per table vertex: inserts its neighbours (duplicate-free) by
+// linear probing from the multiplicative hash slot.
+__global__ void build_hash_kernel(const int64_t *__restrict__ vertex, const int32_t *__restrict__ edge,
+                                  const int32_t *__restrict__ ids, int32_t n_ids, const int64_t *__restrict__ off,
+                                  uint32_t *__restrict__ slots) {
+    const int lane = threadIdx.x & 31;
+    const int64_t warp = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = (static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5;
+    for (int64_t i = warp; i < n_ids; i += nwarps) {
+        const int32_t v = ids[i];
+        uint32_t *t = slots + off[v];
+        const uint32_t cap = static_cast<uint32_t>(off[v + 1] - off[v]);
+        const int bits = __ffs(cap) - 1;
+        for (int64_t j = vertex[v] + lane; j < vertex[v + 1]; j += 32) {
+            const uint32_t x = static_cast<uint32_t>(edge[j]);
+            uint32_t s = (x * 2654435769u) >> (32 - bits);
+            for (uint32_t k = 0; k < cap; ++k) {
+                if (atomicCAS(&t[s], 0xffffffffu, x) == 0xffffffffu) break;
+                s = (s + 1) & (cap - 1);
+            }
+        }
+    }
+}
+}  // namespace
+
+static int build_hash(gi_graph *g, const int64_t *vertex, cudaStream_t st) {
+    size_t budget = kHashBytes;
+    int32_t min_degree = kHashMinDegree;
+    if (const char *s = std::getenv("GI_HASH_MB")) budget = static_cast<size_t>(std::strtoull(s, nullptr, 10)) << 20;
+    if (const char *s = std::getenv("GI_HASH_MIN_DEGREE")) min_degree = std::max(1, std::atoi(s));
+    if (budget == 0 || g->max_degree < min_degree) return GI_OK;
+    // The smallest threshold whose tables fit the budget.
+    std::vector<std::pair<int32_t, int64_t>> big;  // (degree, table slots), largest degree first
+    for (int32_t v = 0; v < g->v_cnt; ++v) {
+        const int64_t d = vertex[v + 1] - vertex[v];
+        if (d >= min_degree) big.emplace_back(static_cast<int32_t>(d), hash_capacity(d));
+    }
+    std::sort(big.begin(), big.end(), [](const auto &a, const auto &b) { return a.first > b.first; });
+    int64_t total = 0;
+    int32_t T = min_degree;
+    for (size_t i = 0; i < big.size(); ++i) {
+        if (static_cast<size_t>(total + big[i].second) * sizeof(uint32_t) > budget) {
+            T = big[i].first + 1;  // this degree and all below are left out
+            break;
+        }
+        total += big[i].second;
+    }
+    if (T > g->max_degree) return GI_OK;
+    std::vector<int64_t> off(static_cast<size_t>(g->v_cnt) + 1, 0);
+    std::vector<int32_t> ids;
+    for (int32_t v = 0; v < g->v_cnt; ++v) {
+        const int64_t d = vertex[v + 1] - vertex[v];
+        const bool has = d >= T;
+        off[v + 1] = off[v] + (has ? hash_capacity(d) : 0);
+        if (has) ids.push_back(v);
+    }
+    const int64_t slots = off[g->v_cnt];
+    int32_t *d_ids = nullptr;
+    cudaError_t e;
+    if ((e = cudaMalloc(&g->d_hash, static_cast<size_t>(slots) * sizeof(uint32_t))) != cudaSuccess ||
+        (e = cudaMalloc(&g->d_hash_off, off.size() * sizeof(int64_t))) != cudaSuccess ||
+        (e = cudaMalloc(&d_ids, ids.size() * sizeof(int32_t))) != cudaSuccess) {
+        cudaFree(d_ids);
+        return cuda_fail(e, "hash table allocation");
+    }
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, g->device);
+    if ((e = cudaMemcpyAsync(g->d_hash_off, off.data(), off.size() * sizeof(int64_t), cudaMemcpyHostToDevice, st)) ==
+            cudaSuccess &&
+        (e = cudaMemcpyAsync(d_ids, ids.data(), ids.size() * sizeof(int32_t), cudaMemcpyHostToDevice, st)) ==
+            cudaSuccess &&
+        (e = cudaMemsetAsync(g->d_hash, 0xff, static_cast<size_t>(slots) * sizeof(uint32_t), st)) == cudaSuccess) {
+        build_hash_kernel<<<sms * 8, 256, 0, st>>>(g->d_vertex, g->d_edge, d_ids, static_cast<int32_t>(ids.size()),
+                                                   g->d_hash_off, g->d_hash);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);  // d_ids is freed next
+    cudaFree(d_ids);
+    if (e != cudaSuccess) return cuda_fail(e, "hash table build");
+    g->hash_min_degree = T;
+    g->hash_slots = slots;
+    return GI_OK;
+}
+
 void cost_model_graph_features(const int64_t *vertex, int32_t v_cnt, int64_t tri_cnt, float *out);
 
 int cuda_fail(cudaError_t e, const char *what) {
@@ -193,6 +293,8 @@ void graph_free(gi_graph *g) {
     cudaFree(g->d_roots);
     cudaFree(g->d_hub_bits);
     cudaFree(g->d_hub_row);
+    cudaFree(g->d_hash);
+    cudaFree(g->d_hash_off);
     cudaSetDevice(prev);
     delete g;
 }
@@ -266,7 +368,8 @@ int graph_create_impl(const int64_t *vertex, const int32_t *edge, int32_t v_cnt,
         graph_free(g);
         return fail(GI_EINVAL, "adjacency lists must be sorted, duplicate-free, in range and without self-loops");
     }
-    const int hub_status = build_hubs(g, vertex, st);
+    int hub_status = build_hubs(g, vertex, st);
+    if (hub_status == GI_OK) hub_status = build_hash(g, vertex, st);
     if (hub_status != GI_OK) {
         graph_free(g);
         return hub_status;
@@ -300,6 +403,8 @@ int gi_graph_get_info(const gi_graph *g, gi_graph_info *o) {
     o->max_intersection_size = g->max_isect;
     o->n_hubs = g->n_hubs;
     o->hub_min_degree = g->hub_min_degree;
+    o->hash_min_degree = g->hash_min_degree;
+    o->hash_slots = g->hash_slots;
     return GI_OK;
 }
 

@@ -170,4 +170,12 @@ struct gi_graph {
     int32_t n_hubs = 0;
     int32_t hub_min_degree = 0x7fffffff;
     int64_t hub_words = 0;
+    // Open-addressing hash sets of the adjacency lists of every vertex of
+    // degree >= hash_min_degree (graph.cu): vertex v's table is
+    // d_hash[d_hash_off[v] .. d_hash_off[v+1]), a power of two at least twice
+    // its degree, empty slots 0xffffffff.  Read by the counting DFS.
+    uint32_t *d_hash = nullptr;
+    int64_t *d_hash_off = nullptr;
+    int32_t hash_min_degree = 0x7fffffff;
+    int64_t hash_slots = 0;
 };
