@@ -262,6 +262,8 @@ class Graph:
         self.max_intersection_size = info.max_intersection_size
         self.n_hubs = info.n_hubs
         self.hub_min_degree = info.hub_min_degree
+        self.hash_min_degree = info.hash_min_degree
+        self.hash_slots = info.hash_slots
 
     @classmethod
     def from_csr(cls, vertex: np.ndarray, edge: np.ndarray, tri_cnt: int = 0, stream: int = 0) -> "Graph":

@@ -490,6 +490,35 @@ struct ListRef {
     int hash_bits;
 };
 
+// Membership of x in a target coded as flat_count codes it: code >= 0 a
+// sorted list tgt[0, code); -1 a bitmap row; <= -2 a hash set of -2 - code
+// bits.
+__device__ __forceinline__ bool member_of(int code, const uint32_t *tgt, uint32_t x) {
+    if (code >= 0) return contains_u32(tgt, code, x);
+    if (code == -1) return ((__ldg(&tgt[x >> 5]) >> (x & 31)) & 1u) != 0;
+    return hash_contains(tgt, -2 - code, x);
+}
+
+// Warp-cooperative a ∩ T for a membership target T (member_of), written to
+// out in a's (sorted) order, or only its size when out is nullptr.
+__device__ __forceinline__ int warp_intersect_probe(const uint32_t *a, int na, int code, const uint32_t *tgt,
+                                                    uint32_t *out, int lane) {
+    int count = 0;
+    for (int base = 0; base < na; base += 32) {
+        const int i = base + lane;
+        uint32_t x = 0;
+        bool found = false;
+        if (i < na) {
+            x = a[i];
+            found = member_of(code, tgt, x);
+        }
+        const unsigned m = __ballot_sync(kFull, found);
+        if (out && found) out[count + __popc(m & ((1u << lane) - 1u))] = x;
+        count += __popc(m);
+    }
+    return count;
+}
+
 // Steps to test one element for membership in l: one bitmap load, about two
 // hash-set loads, or a binary search.
 __device__ __forceinline__ int member_cost(const ListRef &l) {
@@ -656,10 +685,20 @@ struct Ctx {
                 const bool by_f = hf >= 0 && fn >= deg, by_v = !by_f && hv >= 0;
                 uint32_t *out = P.mode[p] == kMaterialize ? slot_base + static_cast<int64_t>(P.slot[p]) * slot_stride
                                                           : nullptr;
+                int bf = 0, bv = 0;
+                const int sf = w.src[f];
+                const uint32_t *tf = by_f || by_v || sf < 0 ? nullptr : hash_table(hashes, sf, fn, bf);
+                const uint32_t *tv = by_f || by_v ? nullptr : hash_table(hashes, v, deg, bv);
+                // A hash set on either side: probe the other list through it
+                // when that takes fewer steps than merging.
+                const int64_t via_v = tv ? 2ll * fn : INT64_MAX, via_f = tf ? 2ll * deg : INT64_MAX;
                 if (by_f)
                     size = warp_intersect_hub(hubs, hf, nb, deg, out, lane);
                 else if (by_v)
                     size = warp_intersect_hub(hubs, hv, fs, fn, out, lane);
+                else if (min(via_v, via_f) < static_cast<int64_t>(fn) + deg)
+                    size = via_v <= via_f ? warp_intersect_probe(fs, fn, -2 - bv, tv, out, lane)
+                                          : warp_intersect_probe(nb, deg, -2 - bf, tf, out, lane);
                 else
                     size = warp_intersect(fs, fn, nb, deg, out, lane);
                 if (lane == 0) {

@@ -67,3 +67,27 @@ def test_batch_applies_tuned_variants():
         counts, lat, _ = b.run()
         assert counts == want
         assert all(x >= 0 for x in lat)
+
+
+def test_membership_structures_do_not_change_counts(monkeypatch):
+    # The same graph with neither hub bitmaps nor hash sets, with hash sets
+    # only, and with both (a low hub threshold): every count and every
+    # variant gives the same raw sum.
+    g = gen.rmat(12, 16.0, 33)
+    graphs = []
+    for hub_mb, hash_mb in ((0, 0), (0, 4096), (64, 4096)):
+        monkeypatch.setenv("GI_HUB_BITMAP_MB", str(hub_mb))
+        monkeypatch.setenv("GI_HUB_MIN_DEGREE", "16")
+        monkeypatch.setenv("GI_HASH_MB", str(hash_mb))
+        dg = gi.Graph.from_csr(g.vertex, g.edge)
+        graphs.append(dg)
+    assert graphs[0].n_hubs == 0 and graphs[0].hash_slots == 0
+    assert graphs[1].n_hubs == 0 and graphs[1].hash_slots > 0 and graphs[1].hash_min_degree == 32
+    assert graphs[2].n_hubs > 0 and graphs[2].hash_slots > 0
+    for n, adj in PATTERNS:
+        s = gi.Schedule_IEP(gi.Pattern(n, adj), g.v_cnt, g.e_cnt, 0)
+        want = gi.pattern_matching(graphs[0], s).raw_sum
+        for flat in (0, 1):
+            s.variant = {"leaf_flat": flat}
+            for dg in graphs:
+                assert gi.pattern_matching(dg, s).raw_sum == want, (adj, flat)
