@@ -11,6 +11,7 @@ valid candidate of a pattern must return the same count: the collector
 records any disagreement.
 
     python -m graphindor_b200.schedule_cost.collect --out runs.json [--budget-ms 400] [--max-s 420]
+        [--light] [--graphs name,name]
 """
 from __future__ import annotations
 
@@ -100,11 +101,15 @@ def main():
     ap.add_argument("--budget-ms", type=float, default=400.0)
     ap.add_argument("--max-s", type=float, default=420.0)
     ap.add_argument("--light", action="store_true", help="the smaller graph set")
+    ap.add_argument("--graphs", default="", help="comma-separated graph names to time (default: all of the set)")
     a = ap.parse_args()
     t_start = time.time()
     pats = pattern_set()
     runs = {"budget_ms": a.budget_ms, "graphs": {}, "rows": []}
+    chosen = set(filter(None, a.graphs.split(",")))
     for gname, make in (LIGHT_GRAPHS if a.light else GRAPHS).items():
+        if chosen and gname not in chosen:
+            continue
         g = make()
         dg = Graph.from_csr(g.vertex, g.edge)
         from .. import clique_count

@@ -9,7 +9,8 @@ smallest predicted time; its regret is time(chosen) / time(fastest measured)
 - 1.  The report compares that regret with the analytic model's own choice
 (the valid candidate of smallest analytic cost).
 
-    python -m graphindor_b200.schedule_cost.train runs.json --out weights.bin [--report report.json]
+    python -m graphindor_b200.schedule_cost.train runs.json [more_runs.json ...] --out weights.bin
+        [--report report.json] [--device gpu]
 
 weights.bin: magic "GIMLP1\\0\\0", int32 dims (in, hidden), then float32
 feature means and scales (in each), W1 (hidden x in), b1, W2 (hidden x
@@ -30,8 +31,24 @@ from .features import DIM, plan_features
 HIDDEN = 128
 
 
-def load_rows(path: str):
-    runs = json.load(open(path))
+def merge_runs(paths):
+    """One runs record from several collections (rows concatenated, graphs
+    united; a row timed out at its own collection's budget)."""
+    out = {"budget_ms": None, "graphs": {}, "rows": []}
+    for p in paths:
+        r = json.load(open(p))
+        out["graphs"].update(r["graphs"])
+        for row in r["rows"]:
+            row = dict(row)
+            if row["ms"] is None:
+                row.setdefault("censored_at_ms", r["budget_ms"])
+            out["rows"].append(row)
+        out["budget_ms"] = r["budget_ms"] if out["budget_ms"] is None else max(out["budget_ms"], r["budget_ms"])
+    return out
+
+
+def load_rows(path):
+    runs = merge_runs(path if isinstance(path, (list, tuple)) else [path])
     budget = runs["budget_ms"]
     gfeat = {k: np.asarray(v["features"], dtype=np.float32) for k, v in runs["graphs"].items()}
     X, y, keys, censored = [], [], [], []
@@ -198,7 +215,7 @@ def split(keys, seed: int = 0):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("runs")
+    ap.add_argument("runs", nargs="+", help="one or more collect.py outputs")
     ap.add_argument("--out", required=True)
     ap.add_argument("--report")
     ap.add_argument("--seed", type=int, default=0)
