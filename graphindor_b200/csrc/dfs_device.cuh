@@ -343,11 +343,25 @@ __device__ __forceinline__ void lane_intersect(const uint32_t *a, int na, const 
     below = need_total ? bel : tot;
 }
 
-// One lane: |a ∩ N(h)| and |a ∩ N(h) ∩ [0, bound)| for a hub h (bitmap row
-// r), one bit test per element of a; with need_total false only elements
-// below bound are tested.  Loads are issued four at a time.
-__device__ __forceinline__ void lane_count_hub(const HubIndex &H, int r, const uint32_t *a, int na, uint32_t bound,
-                                               bool need_total, int &total, int &below) {
+// Membership tests for the counting helpers below: a hub's bitmap row, or
+// an adjacency hash set.
+struct HubTest {
+    const HubIndex &H;
+    int r;
+    __device__ __forceinline__ bool operator()(uint32_t x) const { return hub_test(H, r, x); }
+};
+struct HashTest {
+    const uint32_t *t;
+    int bits;
+    __device__ __forceinline__ bool operator()(uint32_t x) const { return hash_contains(t, bits, x); }
+};
+
+// One lane: |a ∩ T| and |a ∩ T ∩ [0, bound)| for a membership test T, one
+// test per element of a; with need_total false only elements below bound
+// are tested.  Loads are issued four at a time.
+template <class Test>
+__device__ __forceinline__ void lane_count_member(const Test &test, const uint32_t *a, int na, uint32_t bound,
+                                                  bool need_total, int &total, int &below) {
     int tot = 0, bel = 0;
     int i = 0;
     for (; i + 4 <= na; i += 4) {
@@ -356,14 +370,14 @@ __device__ __forceinline__ void lane_count_hub(const HubIndex &H, int r, const u
             na = i;  // sorted: nothing further is below bound
             break;
         }
-        const bool h0 = hub_test(H, r, x0), h1 = hub_test(H, r, x1), h2 = hub_test(H, r, x2), h3 = hub_test(H, r, x3);
+        const bool h0 = test(x0), h1 = test(x1), h2 = test(x2), h3 = test(x3);
         tot += h0 + h1 + h2 + h3;
         bel += (h0 && x0 < bound) + (h1 && x1 < bound) + (h2 && x2 < bound) + (h3 && x3 < bound);
     }
     for (; i < na; ++i) {
         const uint32_t x = a[i];
         if (!need_total && x >= bound) break;
-        const bool h = hub_test(H, r, x);
+        const bool h = test(x);
         tot += h;
         bel += h && x < bound;
     }
@@ -371,14 +385,15 @@ __device__ __forceinline__ void lane_count_hub(const HubIndex &H, int r, const u
     below = bel;
 }
 
-// Warp-cooperative |a ∩ N(h)| and |a ∩ N(h) ∩ [0, bound)| (warp-uniform).
-__device__ __forceinline__ void warp_count_hub(const HubIndex &H, int r, const uint32_t *a, int na, uint32_t bound,
-                                               bool need_total, int lane, int &total, int &below) {
+// Warp-cooperative |a ∩ T| and |a ∩ T ∩ [0, bound)| (warp-uniform).
+template <class Test>
+__device__ __forceinline__ void warp_count_member(const Test &test, const uint32_t *a, int na, uint32_t bound,
+                                                  bool need_total, int lane, int &total, int &below) {
     if (!need_total) na = lower_bound_u32(a, na, bound);
     int t = 0, u = 0;
     for (int i = lane; i < na; i += 32) {
         const uint32_t x = a[i];
-        if (hub_test(H, r, x)) {
+        if (test(x)) {
             ++t;
             u += x < bound;
         }
@@ -819,16 +834,35 @@ struct Ctx {
                 const bool need_total = kBytesOn || !(last_level && p == L);
                 const int hf = w.hub[f];
                 int tot, bel;
+                // A hash set on either side (when no bitmap serves): probe
+                // the other list through it if that takes fewer steps.
+                int bf = 0, bv = 0;
+                const uint32_t *tf = nullptr, *tv = nullptr;
+                if (!(hf >= 0 && fn >= dv) && hv < 0) {
+                    if (w.src[f] >= 0) tf = hash_table(hashes, static_cast<uint32_t>(w.src[f]), fn, bf);
+                    tv = hash_table(hashes, v, dv, bv);
+                }
+                const int merge_steps = kWarp ? (fn + dv + 31) / 32 : lane_cost(fn, dv);
+                const int via_v = tv ? 2 * fn / (kWarp ? 32 : 1) : 0x7fffffff;
+                const int via_f = tf ? 2 * dv / (kWarp ? 32 : 1) : 0x7fffffff;
                 if (hf >= 0 && fn >= dv) {
                     if (kWarp)
-                        warp_count_hub(hubs, hf, nv, dv, bound, need_total, lane, tot, bel);
+                        warp_count_member(HubTest{hubs, hf}, nv, dv, bound, need_total, lane, tot, bel);
                     else
-                        lane_count_hub(hubs, hf, nv, dv, bound, need_total, tot, bel);
+                        lane_count_member(HubTest{hubs, hf}, nv, dv, bound, need_total, tot, bel);
                 } else if (hv >= 0) {
                     if (kWarp)
-                        warp_count_hub(hubs, hv, fs, fn, bound, need_total, lane, tot, bel);
+                        warp_count_member(HubTest{hubs, hv}, fs, fn, bound, need_total, lane, tot, bel);
                     else
-                        lane_count_hub(hubs, hv, fs, fn, bound, need_total, tot, bel);
+                        lane_count_member(HubTest{hubs, hv}, fs, fn, bound, need_total, tot, bel);
+                } else if (min(via_v, via_f) < merge_steps) {
+                    const bool probe_f = via_v <= via_f;  // fs's elements into N(v)'s set
+                    const HashTest test{probe_f ? tv : tf, probe_f ? bv : bf};
+                    if (kWarp)
+                        warp_count_member(test, probe_f ? fs : nv, probe_f ? fn : dv, bound, need_total, lane, tot,
+                                          bel);
+                    else
+                        lane_count_member(test, probe_f ? fs : nv, probe_f ? fn : dv, bound, need_total, tot, bel);
                 } else if (kWarp) {
                     warp_count2(fs, fn, nv, dv, bound, need_total, lane, tot, bel);
                 } else {
@@ -932,13 +966,19 @@ struct Ctx {
                 if (!used && !(P.vertex_induced && anti_adjacent(P, w, D, v, vertex, edge))) {
                     const int dv = static_cast<int>(__ldg(&vertex[v + 1]) - __ldg(&vertex[v]));
                     const bool v_hub = dv >= hubs.min_degree;
+                    const bool v_hash = dv >= hashes.min_degree;
                     int cost = 0;
                     for (int p = P.last[D]; p != -1; p = P.next[p]) {
                         const int f = P.father[p];
                         if (f < 0) continue;
                         const int fn = w.set_size[f];
-                        // bitmap tests: one step per element of the other list
-                        cost += w.hub[f] >= 0 && fn >= dv ? dv : v_hub ? fn : lane_cost(fn, dv);
+                        // bitmap tests: one step per element of the other
+                        // list; hash-set probes about two
+                        const bool f_hash = w.src[f] >= 0 && fn >= hashes.min_degree;
+                        int c = w.hub[f] >= 0 && fn >= dv ? dv : v_hub ? fn : lane_cost(fn, dv);
+                        if (v_hash) c = min(c, 2 * fn);
+                        if (f_hash) c = min(c, 2 * dv);
+                        cost += c;
                     }
                     heavy = cost > (kLaneBudgetOverride >= 0 ? kLaneBudgetOverride : P.lane_budget);
                     if (!heavy) acc += leaf_eval<false>(D, v);
