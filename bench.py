@@ -91,6 +91,7 @@ def parse_args():
                     help="divides every edge step (a larger sample); 1 = the pinned subsets")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-vs-model block")
+    ap.add_argument("--no-tune", action="store_true", help="default kernel variants instead of autotuned ones")
     ap.add_argument("--learned-graphs", type=int, default=16)
     ap.add_argument("--learned-patterns", type=int, default=48)
     return ap.parse_args()
@@ -181,9 +182,20 @@ def run_ours(args, world, rank, local):
     names = [n for n, _, _ in PATTERNS]
 
     def plan_all(graph):
-        return {name: gi.Schedule_IEP(gi.Pattern(n, adj), graph.v_cnt, graph.e_cnt, tri) for name, n, adj in PATTERNS}
+        out = {name: gi.Schedule_IEP(gi.Pattern(n, adj), graph.v_cnt, graph.e_cnt, tri) for name, n, adj in PATTERNS}
+        if not args.no_tune:  # the autotuner's cached variant of each plan's class
+            for name, p in out.items():  # its sample starts at the size of the pattern's subset here
+                gi.autotune(graph, p, sample_edges=max(1, graph.e_cnt // steps_p[name]), max_ms=400.0,
+                            stream=sid)
+        return out
 
+    # Kernel variants: the autotuner times them once per class of (plan,
+    # graph) on its own edge sample, untimed; later plans take the cached
+    # choice (inside the end-to-end region below as well).
+    t_tune = time.perf_counter()
     plans = plan_all(dg)
+    tune_s = time.perf_counter() - t_tune
+    variants = {name: plans[name].variant for name in names}
     divisors = {name: plans[name].export()["count_divisor"] for name in names}
 
     def one_step(graph, plan_map, acc, count_bytes=False):
@@ -287,6 +299,8 @@ def run_ours(args, world, rank, local):
             "embeddings_per_s": {n: emb[n] / max(1e-9, (acc[n]["kernel_ms"] + acc[n]["prep_ms"]) / args.steps / 1e3)
                                  for n in names},
             "patterns": {n: adj for n, _, adj in PATTERNS},
+            "kernel_variants": variants,
+            "tuning_s": tune_s,
             "l2": "inputs larger than L2 (CSR %.2f GB vs 126 MB)" % ((g.vertex.nbytes + g.edge.nbytes) / 1e9),
             "parallelism": f"dp{world}: the subset's work chunks interleaved across ranks",
         },

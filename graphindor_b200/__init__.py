@@ -134,14 +134,13 @@ class Schedule_IEP:
         """The plan's kernel variant (speed only, never counts)."""
         v = N.Variant()
         check(lib().gi_plan_get_variant(self._h, C.byref(v)), "gi_plan_get_variant")
-        return {"leaf_flat": v.leaf_flat, "lane_budget": v.lane_budget, "occupancy": v.occupancy}
+        return {k: getattr(v, k) for k, _ in N.Variant._fields_}
 
     @variant.setter
     def variant(self, v: dict) -> None:
         cur = self.variant
         cur.update(v)
-        check(lib().gi_plan_set_variant(self._h, C.byref(N.Variant(cur["leaf_flat"], cur["lane_budget"],
-                                                                    cur["occupancy"]))), "gi_plan_set_variant")
+        check(lib().gi_plan_set_variant(self._h, C.byref(N.Variant(**cur))), "gi_plan_set_variant")
 
     @classmethod
     def learned(cls, pattern: Pattern, graph: "Graph", enable_iep: bool = True,
@@ -199,7 +198,7 @@ def autotune(graph: "Graph", schedule: Schedule_IEP, *, sample_edges: int = 0, m
     check(lib().gi_autotune(graph.handle, schedule.handle, C.c_void_p(stream) if stream else None, C.byref(o),
                             C.byref(info)), "gi_autotune")
     c = info.chosen
-    return {"chosen": {"leaf_flat": c.leaf_flat, "lane_budget": c.lane_budget, "occupancy": c.occupancy},
+    return {"chosen": {k: getattr(c, k) for k, _ in N.Variant._fields_},
             "cached": bool(info.cached), "candidates": info.candidates, "best_ms": info.best_ms,
             "default_ms": info.default_ms, "sample_edges": info.sample_edges}
 

@@ -57,6 +57,9 @@ void variant_apply(DevPlan &P, const gi_variant &v) {
     P.flat_first = P.leaf_flat && P.flat_first_ok;
     if (v.lane_budget > 0) P.lane_budget = v.lane_budget;
     P.occupancy = v.occupancy;
+    P.split = v.split;
+    P.leaf_handoff = v.leaf_handoff;
+    P.mid_handoff = v.mid_handoff;
 }
 
 gi_variant variant_of(const DevPlan &P) {
@@ -64,6 +67,9 @@ gi_variant variant_of(const DevPlan &P) {
     v.leaf_flat = P.leaf_flat;
     v.lane_budget = P.lane_budget;
     v.occupancy = P.occupancy;
+    v.split = P.split;
+    v.leaf_handoff = P.leaf_handoff;
+    v.mid_handoff = P.mid_handoff;
     return v;
 }
 
@@ -94,6 +100,8 @@ int gi_plan_set_variant(gi_plan *p, const gi_variant *v) {
     if (v->occupancy != 0 && v->occupancy != 1 && v->occupancy != 16)
         return fail(GI_EINVAL, "occupancy must be 0, 1 or 16");
     if (v->lane_budget < 0) return fail(GI_EINVAL, "lane_budget must be >= 0");
+    if (v->split < 0 || v->split > (1 << 20) || v->leaf_handoff < 0 || v->mid_handoff < 0)
+        return fail(GI_EINVAL, "split, leaf_handoff and mid_handoff must be >= 0 (split at most 2^20)");
     variant_apply(p->dev, *v);
     return GI_OK;
 }
@@ -146,21 +154,14 @@ int gi_autotune(const gi_graph *g, gi_plan *p, gi_stream stream, const gi_tune_o
         }
         break;
     }
-    const int budgets[2] = {256, 2048};
-    std::vector<gi_variant> cands;
-    for (int occ : {1, 16}) {
-        cands.push_back(gi_variant{1, original.lane_budget, occ});
-        for (int b : budgets) cands.push_back(gi_variant{0, b, occ});
-    }
-    double best = INFINITY;
-    gi_variant chosen = variant_of(original);
+    // Times variant v on the sample (the fastest of o.reps runs; INFINITY
+    // when it runs past max_ms) and checks its raw sum against the others.
     bool have_sum = false;
     uint64_t sum = 0;
-    int st = GI_OK;
-    for (const gi_variant &v : cands) {
+    auto time_variant = [&](const gi_variant &v, double &t) -> int {
         p->dev = original;
         variant_apply(p->dev, v);
-        double t = INFINITY;
+        t = INFINITY;
         for (int r = 0; r < o.reps; ++r) {
             gi_stats s{};
             s.edge_step = step;
@@ -169,26 +170,61 @@ int gi_autotune(const gi_graph *g, gi_plan *p, gi_stream stream, const gi_tune_o
             uint64_t raw = 0;
             const int rc = gi_count_shard(g, p, 0, 1, stream, &raw, &s);
             if (rc == GI_ETIMEOUT) break;  // slower than max_ms: not a candidate
-            if (rc != GI_OK) {
-                st = rc;
-                break;
-            }
-            if (have_sum && raw != sum) {
-                st = fail(GI_ECUDA, "kernel variants counted the same sample differently");
-                break;
-            }
+            if (rc != GI_OK) return rc;
+            if (have_sum && raw != sum) return fail(GI_ECUDA, "kernel variants counted the same sample differently");
             sum = raw;
             have_sum = true;
             t = std::min(t, s.kernel_ms + s.prep_ms);
         }
-        if (st != GI_OK) break;
         ++res.candidates;
-        if (v.leaf_flat == original.leaf_flat && v.lane_budget == original.lane_budget &&
-            v.occupancy == (original.occupancy ? original.occupancy : (original.n >= 6 ? 16 : 1)))
+        return GI_OK;
+    };
+    double best = INFINITY;
+    gi_variant chosen = variant_of(original);
+    int st = GI_OK;
+    // Stage 1: the leaf level and the occupancy.
+    const int budgets[2] = {256, 2048};
+    std::vector<gi_variant> cands;
+    for (int occ : {1, 16}) {
+        cands.push_back(gi_variant{1, original.lane_budget, occ, 0, 0, 0});
+        for (int b : budgets) cands.push_back(gi_variant{0, b, occ, 0, 0, 0});
+    }
+    const int default_occ = original.occupancy ? original.occupancy : (original.n >= 6 ? 16 : 1);
+    for (const gi_variant &v : cands) {
+        double t;
+        if ((st = time_variant(v, t)) != GI_OK) break;
+        if (v.leaf_flat == original.leaf_flat && v.lane_budget == original.lane_budget && v.occupancy == default_occ)
             res.default_ms = t;
         if (t < best) {
             best = t;
             chosen = v;
+        }
+    }
+    // Stage 2: the work split of the depth-2 loop (a quarter and four times
+    // the default), then stage 3: the leaf donation threshold.
+    if (st == GI_OK && original.loop2_kind >= 0) {
+        const int d = original.leaf_depth == 2 ? 256 : 32;
+        for (int sp : {d / 4, d * 4}) {
+            gi_variant v = chosen;
+            v.split = sp;
+            double t;
+            if ((st = time_variant(v, t)) != GI_OK) break;
+            if (t < best) {
+                best = t;
+                chosen = v;
+            }
+        }
+    }
+    if (st == GI_OK && original.leaf_depth >= 2) {
+        for (int lh : {16, 256}) {
+            gi_variant v = chosen;
+            v.leaf_handoff = lh;
+            double t;
+            if ((st = time_variant(v, t)) != GI_OK) break;
+            if (t < best) {
+                best = t;
+                chosen = v;
+            }
         }
     }
     p->dev = original;

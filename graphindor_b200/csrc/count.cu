@@ -243,7 +243,10 @@ int ensure_scratch(gi_graph *g, size_t bytes) {
 #ifndef GI_SPLIT_DEEP
 #define GI_SPLIT_DEEP 32
 #endif
-static int split_size(const DevPlan &P) { return P.leaf_depth == 2 ? GI_SPLIT_LEAF2 : GI_SPLIT_DEEP; }
+static int split_size(const DevPlan &P) {
+    if (P.split > 0) return P.split;
+    return P.leaf_depth == 2 ? GI_SPLIT_LEAF2 : GI_SPLIT_DEEP;
+}
 
 // Builds the subtask offsets for the plan's depth-2 split; returns the
 // number of subtasks.  Caller holds g->mu.

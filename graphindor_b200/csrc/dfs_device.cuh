@@ -952,7 +952,7 @@ struct Ctx {
         unsigned long long acc = 0;
         for (int base = i0; base < i1; base += 32) {
             if (out_of_time()) break;
-            if (hq.items && i1 - base >= 2 * kLeafHandoffMin) {
+            if (hq.items && i1 - base >= 2 * (P.leaf_handoff > 0 ? P.leaf_handoff : kLeafHandoffMin)) {
                 const int mid = base + ((i1 - base) / 2 + 31) / 32 * 32;
                 if (mid < i1 && donate(D, mid, i1)) i1 = mid;
             }
@@ -1153,7 +1153,7 @@ struct Ctx {
         unsigned long long acc = 0;
         for (int base = i0; base < i1; base += 32) {
             if (out_of_time()) break;
-            if (hq.items && i1 - base >= 2 * kLeafHandoffMin) {
+            if (hq.items && i1 - base >= 2 * (P.leaf_handoff > 0 ? P.leaf_handoff : kLeafHandoffMin)) {
                 const int mid = base + ((i1 - base) / 2 + 31) / 32 * 32;
                 if (mid < i1 && donate(D, mid, i1)) i1 = mid;
             }
@@ -1248,7 +1248,7 @@ struct Ctx {
             int i = w.cursor[d];
             bool descended = false;
             while (i < ns) {
-                if (hq.items && ns - i >= 2 * kMidHandoffMin) {
+                if (hq.items && ns - i >= 2 * (P.mid_handoff > 0 ? P.mid_handoff : kMidHandoffMin)) {
                     const int mid = i + (ns - i + 1) / 2;
                     if (donate(d, mid, ns)) {
                         ns = mid;

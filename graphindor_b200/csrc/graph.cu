@@ -78,10 +78,13 @@ __global__ void build_hub_bits_kernel(const int64_t *__restrict__ vertex, const 
 
 // Hub bitmaps: the counting DFS tests membership in a hub's adjacency list
 // with one load.  Hubs are all vertices of degree >= T, T the smallest value
-// >= kHubMinDegree for which their bitmaps fit kHubBitmapBytes.
+// >= kHubMinDegree for which their bitmaps fit the budget: kHubBitmapBytes,
+// at most a sixteenth of the device's free memory.  Measured on the B200 (R-MAT
+// scale 22, the six-pattern workload): 64 MiB 3.69 s per step, 1 GiB 2.93 s,
+// 4 GiB 2.39 s.
 int cuda_fail(cudaError_t e, const char *what);
 
-constexpr size_t kHubBitmapBytes = size_t(64) << 20;
+constexpr size_t kHubBitmapBytes = size_t(4) << 30;
 constexpr int32_t kHubMinDegree = 256;
 
 // The bitmap budget in bytes and the smallest hub degree: the defaults
@@ -89,6 +92,8 @@ constexpr int32_t kHubMinDegree = 256;
 // (tuning; 0 MB turns the bitmaps off).
 static void hub_limits(size_t &bytes, int32_t &min_degree) {
     bytes = kHubBitmapBytes;
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) bytes = std::min(bytes, free_b / 16);
     min_degree = kHubMinDegree;
     if (const char *s = std::getenv("GI_HUB_BITMAP_MB")) bytes = static_cast<size_t>(std::strtoull(s, nullptr, 10)) << 20;
     if (const char *s = std::getenv("GI_HUB_MIN_DEGREE")) min_degree = std::max(1, std::atoi(s));
@@ -145,9 +150,13 @@ static int build_hubs(gi_graph *g, const int64_t *vertex, cudaStream_t st) {
 // one or two loads instead of a binary search of log2 d(v) dependent loads.
 // Every vertex of degree >= T gets a table of next_pow2(2 d(v)) slots (load
 // at most 1/2, linear probing); T is the smallest value >= kHashMinDegree
-// for which all tables fit the budget (GI_HASH_MB, default kHashBytes; 0
-// turns them off; GI_HASH_MIN_DEGREE overrides kHashMinDegree).
-constexpr size_t kHashBytes = size_t(4) << 30;
+// for which all tables fit the budget (GI_HASH_MB, default kHashBytes;
+// GI_HASH_MIN_DEGREE overrides kHashMinDegree).  Off by default: with the
+// default hub bitmaps they did not shorten the six-pattern workload at R-MAT
+// scale 22 on the B200 (2.385 s per step with 4 GiB of them, 2.386 s without)
+// and cost 100 ms of upload; they pay where the bitmap budget is small
+// (64 MiB of bitmaps: 3.57 s with them, 3.69 s without).
+constexpr size_t kHashBytes = 0;
 constexpr int32_t kHashMinDegree = 32;
 
 int64_t hash_capacity(int64_t deg) {

@@ -71,6 +71,9 @@ struct DevPlan {
     int32_t flat_first;         // 1: the DFS ends at depth 2 and a chunk's edges are counted as one flat leaf
     int32_t flat_first_ok;      // the plan allows flat_first (set with leaf_flat)
     int32_t occupancy;          // resident blocks per SM the kernel is built for: 0 by pattern size, 1 or 16
+    int32_t split;              // depth-2 candidates per subtask (0: 256 when depth 2 is the leaf, else 32)
+    int32_t leaf_handoff;       // leaf ranges of at least twice this are donated (0: 64)
+    int32_t mid_handoff;        // intermediate ranges of at least twice this are donated (0: 4)
     int32_t loop2_kind;         // bound of the depth-2 loop set: 0 d(v0), 1 d(v1), 2 min, -1 none
     int32_t pdepth[GI_MAX_PREFIX];  // last member (position) of each prefix
     int32_t father[GI_MAX_PREFIX];

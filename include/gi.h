@@ -248,6 +248,9 @@ typedef struct gi_variant {
     int32_t leaf_flat;   /* 1: leaf probes spread evenly over a warp's lanes; 0: a candidate per lane */
     int32_t lane_budget; /* leaf_flat 0: candidates costlier than this run on the whole warp (0 = keep) */
     int32_t occupancy;   /* resident blocks per SM the kernel is built for: 1, 16, or 0 = by pattern size */
+    int32_t split;       /* depth-2 candidates per work item (0 = 256 when depth 2 is the leaf, else 32) */
+    int32_t leaf_handoff; /* leaf loop ranges of at least twice this go to idle warps (0 = 64) */
+    int32_t mid_handoff; /* intermediate loop ranges of at least twice this go to idle warps (0 = 4) */
 } gi_variant;
 int gi_plan_get_variant(const gi_plan *p, gi_variant *out);
 int gi_plan_set_variant(gi_plan *p, const gi_variant *v);

@@ -27,6 +27,9 @@ def test_every_variant_counts_the_same():
                 for occ in (0, 1, 16):
                     s.variant = {"leaf_flat": flat, "lane_budget": budget, "occupancy": occ}
                     assert gi.pattern_matching(dg, s).raw_sum == want, (adj, flat, budget, occ)
+        for split, lh, mh in ((1, 1, 1), (8, 16, 2), (1024, 256, 64)):
+            s.variant = {"split": split, "leaf_handoff": lh, "mid_handoff": mh}
+            assert gi.pattern_matching(dg, s).raw_sum == want, (adj, split, lh, mh)
         # Edge subsets too (the tuner's sample).
         s.variant = {"leaf_flat": 1, "occupancy": 16}
         tot = sum(gi.count_edges(dg, s, 5, off).raw_sum for off in range(5)) % (1 << 64)
@@ -41,10 +44,9 @@ def test_tuner_picks_a_timed_variant_and_caches_it():
         s = gi.Schedule_IEP(gi.Pattern(n, adj), g.v_cnt, g.e_cnt, 0)
         want = gi.pattern_matching(dg, s).raw_sum
         info = gi.autotune(dg, s, sample_edges=4096)
-        assert not info["cached"] and info["candidates"] == 6
+        assert not info["cached"] and 6 <= info["candidates"] <= 10
         assert info["best_ms"] > 0 and info["best_ms"] <= info["default_ms"] + 1e-9
-        assert s.variant["leaf_flat"] == info["chosen"]["leaf_flat"]
-        assert s.variant["occupancy"] == info["chosen"]["occupancy"]
+        assert s.variant == info["chosen"]
         assert gi.pattern_matching(dg, s).raw_sum == want
         s2 = gi.Schedule_IEP(gi.Pattern(n, adj), g.v_cnt, g.e_cnt, 0)
         again = gi.autotune(dg, s2)
