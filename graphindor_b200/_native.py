@@ -80,7 +80,7 @@ class Stats(C.Structure):
 
 class Variant(C.Structure):
     _fields_ = [("leaf_flat", C.c_int32), ("lane_budget", C.c_int32), ("occupancy", C.c_int32), ("split", C.c_int32),
-                ("leaf_handoff", C.c_int32), ("mid_handoff", C.c_int32)]
+                ("leaf_handoff", C.c_int32), ("mid_handoff", C.c_int32), ("edge_triangles", C.c_int32)]
 
 
 class TuneOptions(C.Structure):

@@ -60,6 +60,7 @@ void variant_apply(DevPlan &P, const gi_variant &v) {
     P.split = v.split;
     P.leaf_handoff = v.leaf_handoff;
     P.mid_handoff = v.mid_handoff;
+    P.tri_edge = v.edge_triangles && P.tri_ok ? 1 : 0;
 }
 
 gi_variant variant_of(const DevPlan &P) {
@@ -70,6 +71,7 @@ gi_variant variant_of(const DevPlan &P) {
     v.split = P.split;
     v.leaf_handoff = P.leaf_handoff;
     v.mid_handoff = P.mid_handoff;
+    v.edge_triangles = P.tri_edge;
     return v;
 }
 
@@ -186,9 +188,10 @@ int gi_autotune(const gi_graph *g, gi_plan *p, gi_stream stream, const gi_tune_o
     const int budgets[2] = {256, 2048};
     std::vector<gi_variant> cands;
     for (int occ : {1, 16}) {
-        cands.push_back(gi_variant{1, original.lane_budget, occ, 0, 0, 0});
-        for (int b : budgets) cands.push_back(gi_variant{0, b, occ, 0, 0, 0});
+        cands.push_back(gi_variant{1, original.lane_budget, occ, 0, 0, 0, 0});
+        for (int b : budgets) cands.push_back(gi_variant{0, b, occ, 0, 0, 0, 0});
     }
+    if (original.tri_ok) cands.push_back(gi_variant{0, original.lane_budget, 0, 0, 0, 0, 1});
     const int default_occ = original.occupancy ? original.occupancy : (original.n >= 6 ? 16 : 1);
     for (const gi_variant &v : cands) {
         double t;

@@ -118,6 +118,16 @@ static int build_dev_plan(const Schedule_IEP &s, DevPlan &d) {
     d.flat_first = d.leaf_flat && d.flat_first_ok;
     d.occupancy = 0;
     for (int p = 0; p < GI_MAX_PREFIX; ++p) d.pdepth[p] = p < tp ? s.get_prefix_data(p).back() : -1;
+    // Edge-triangle counting (tri_edge.cu) serves plans whose DFS ends at
+    // depth 2 in an IEP tail and whose sets before it are N(v0), N(v1) and
+    // N(v0) ∩ N(v1) only.
+    d.tri_ok = d.iep_k > 0 && d.stop == 2 && !d.vertex_induced;
+    for (int p = 0; p < tp && d.tri_ok; ++p) {
+        const int f = d.father[p];
+        if (d.pdepth[p] == 0 && f != -1) d.tri_ok = 0;
+        if (d.pdepth[p] == 1 && f != -1 && (d.pdepth[f] != 0 || d.father[f] != -1)) d.tri_ok = 0;
+    }
+    d.tri_edge = 0;
     // Splitting of the depth-2 loop: its set's members are a subset of {0, 1}.
     d.loop2_kind = -1;
     if (d.stop > 2 && d.loop_set[2] >= 0) {

@@ -85,6 +85,8 @@ __global__ void oriented_fill_kernel(const int64_t *__restrict__ vertex, const i
     }
 }
 
+}  // namespace
+
 // Builds (once) and caches the oriented DAG of g.  Caller holds g->mu.
 int oriented_graph(gi_graph *g, int orientation, cudaStream_t st, gi_graph **out) {
     if (g->oriented[orientation]) {
@@ -154,6 +156,8 @@ int oriented_graph(gi_graph *g, int orientation, cudaStream_t st, gi_graph **out
     *out = o;
     return GI_OK;
 }
+
+namespace {
 
 std::string clique_adj(int k) {
     std::string s(static_cast<size_t>(k) * k, '1');

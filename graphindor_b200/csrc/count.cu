@@ -299,6 +299,9 @@ DfsKernel pick_dfs_kernel(bool bytes_on, const DevPlan &P) {
     return deep ? dfs_count_kernel<false, 16> : dfs_count_kernel<false, 1>;
 }
 
+int count_tri_edge(gi_graph *g, const DevPlan &P, cudaStream_t st, int64_t edge_step, int64_t edge_offset,
+                   int64_t shard, int64_t num_shards, uint64_t *raw_sum, gi_stats *stats);
+
 // Runs the counting kernel for one plan on one graph (or one shard of it).
 // budget_ms = 0 means no budget.
 int count_impl(gi_graph *g, const DevPlan &plan, cudaStream_t st, uint64_t *raw_sum, gi_stats *stats,
@@ -312,6 +315,10 @@ int count_impl(gi_graph *g, const DevPlan &plan, cudaStream_t st, uint64_t *raw_
     const int64_t edge_step = stats && stats->edge_step > 1 ? stats->edge_step : 1;
     const int64_t edge_offset = edge_step > 1 ? stats->edge_offset : 0;
     if (edge_offset < 0 || edge_offset >= edge_step) return fail(GI_EINVAL, "edge_offset outside [0, edge_step)");
+    // The edge-triangle path (tri_edge.cu) for plans that allow it, except
+    // for the instrumented, time-budgeted-sample and fixed-sample modes.
+    if (P.tri_edge && P.tri_ok && !bytes_on && !(stats && (stats->allow_partial || stats->sample_chunks > 0)))
+        return count_tri_edge(g, P, st, edge_step, edge_offset, shard, num_shards, raw_sum, stats);
     cudaError_t e;
     const auto kernel = pick_dfs_kernel(bytes_on, P);
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, kernel, kBlockThreads, 0);

@@ -304,6 +304,7 @@ void graph_free(gi_graph *g) {
     cudaFree(g->d_hub_row);
     cudaFree(g->d_hash);
     cudaFree(g->d_hash_off);
+    cudaFree(g->d_tri_arc);
     cudaSetDevice(prev);
     delete g;
 }

@@ -74,6 +74,8 @@ struct DevPlan {
     int32_t split;              // depth-2 candidates per subtask (0: 256 when depth 2 is the leaf, else 32)
     int32_t leaf_handoff;       // leaf ranges of at least twice this are donated (0: 64)
     int32_t mid_handoff;        // intermediate ranges of at least twice this are donated (0: 4)
+    int32_t tri_ok;             // the plan can be counted from edge-triangle counts (tri_edge.cu)
+    int32_t tri_edge;           // 1: count it that way (a variant; needs tri_ok)
     int32_t loop2_kind;         // bound of the depth-2 loop set: 0 d(v0), 1 d(v1), 2 min, -1 none
     int32_t pdepth[GI_MAX_PREFIX];  // last member (position) of each prefix
     int32_t father[GI_MAX_PREFIX];
@@ -181,4 +183,8 @@ struct gi_graph {
     int64_t *d_hash_off = nullptr;
     int32_t hash_min_degree = 0x7fffffff;
     int64_t hash_slots = 0;
+    // Per-arc triangle counts of the degree-oriented DAG (tri_edge.cu),
+    // recomputed by every edge-triangle count; the buffer is kept.
+    void *d_tri_arc = nullptr;
+    int64_t tri_arc_cap = 0;
 };

@@ -251,6 +251,9 @@ typedef struct gi_variant {
     int32_t split;       /* depth-2 candidates per work item (0 = 256 when depth 2 is the leaf, else 32) */
     int32_t leaf_handoff; /* leaf loop ranges of at least twice this go to idle warps (0 = 64) */
     int32_t mid_handoff; /* intermediate loop ranges of at least twice this go to idle warps (0 = 4) */
+    int32_t edge_triangles; /* 1: count from per-edge triangle counts of the degree-oriented DAG; only
+                               for plans ending at depth 2 in an IEP tail over N(v0), N(v1) and
+                               N(v0) ∩ N(v1) (the diamond, books), else ignored */
 } gi_variant;
 int gi_plan_get_variant(const gi_plan *p, gi_variant *out);
 int gi_plan_set_variant(gi_plan *p, const gi_variant *v);

@@ -25,3 +25,13 @@ def test_variant_round_trip_and_validation():
     with pytest.raises(gi.GIError):
         s.variant = {"split": -2}
     assert s.export() == before
+
+
+def test_edge_triangle_variant_only_for_plans_that_allow_it():
+    d = gi.Schedule_IEP(gi.Pattern(4, "0111101111001100"), 1 << 16, 1 << 20, 1 << 18)  # diamond
+    d.variant = {"edge_triangles": 1}
+    assert d.variant["edge_triangles"] == 1
+    for n, adj in ((4, "0110100110010110"), (3, "011101110"), (5, "0101110101010101010011000")):
+        s = gi.Schedule_IEP(gi.Pattern(n, adj), 1 << 16, 1 << 20, 1 << 18)
+        s.variant = {"edge_triangles": 1}
+        assert s.variant["edge_triangles"] == 0, adj

@@ -93,3 +93,37 @@ def test_membership_structures_do_not_change_counts(monkeypatch):
             s.variant = {"leaf_flat": flat}
             for dg in graphs:
                 assert gi.pattern_matching(dg, s).raw_sum == want, (adj, flat)
+
+
+def _adj(n, edges):
+    m = [[0] * n for _ in range(n)]
+    for a, b in edges:
+        m[a][b] = m[b][a] = 1
+    return "".join(str(m[i][j]) for i in range(n) for j in range(n))
+
+
+# Plans that end at depth 2 in an IEP tail over N(v0), N(v1), N(v0) ∩ N(v1).
+EDGE_TRIANGLE_PATTERNS = [(4, "0111101111001100"),  # diamond
+                          (5, _adj(5, [(0, 1), (0, 2), (1, 2), (0, 3), (1, 3), (0, 4), (1, 4)])),  # 3-book
+                          (6, _adj(6, [(0, 1)] + [(0, k) for k in range(2, 6)] + [(1, k) for k in range(2, 6)])),
+                          (4, _adj(4, [(0, 1), (1, 2), (0, 2), (0, 3)]))]  # tailed triangle
+
+
+def test_edge_triangle_path_counts_like_the_dfs():
+    for g in (gen.rmat(12, 16.0, 34), gen.chung_lu(3000, 60000, 2.0, 800.0, 35), gen.erdos_renyi(500, 9000, 36)):
+        dg = gi.Graph.from_csr(g.vertex, g.edge)
+        for n, adj in EDGE_TRIANGLE_PATTERNS:
+            s = gi.Schedule_IEP(gi.Pattern(n, adj), g.v_cnt, g.e_cnt, 0)
+            want = gi.pattern_matching(dg, s)
+            subsets = [gi.count_edges(dg, s, 7, off).raw_sum for off in (0, 3, 6)]
+            shards = [gi.count_edges(dg, s, 3, 1, shard=k, num_shards=2).raw_sum for k in (0, 1)]
+            s.variant = {"edge_triangles": 1}
+            assert s.variant["edge_triangles"] == 1
+            got = gi.pattern_matching(dg, s)
+            assert (got.raw_sum, got.count, got.tasks) == (want.raw_sum, want.count, want.tasks), adj
+            assert [gi.count_edges(dg, s, 7, off).raw_sum for off in (0, 3, 6)] == subsets, adj
+            assert [gi.count_edges(dg, s, 3, 1, shard=k, num_shards=2).raw_sum for k in (0, 1)] == shards, adj
+    # A plan that does not qualify keeps the general kernel.
+    s = gi.Schedule_IEP(gi.Pattern(4, "0110100110010110"), 100, 1000, 0)
+    s.variant = {"edge_triangles": 1}
+    assert s.variant["edge_triangles"] == 0
