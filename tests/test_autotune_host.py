@@ -15,7 +15,7 @@ def test_variant_round_trip_and_validation():
     assert v["split"] == v["leaf_handoff"] == v["mid_handoff"] == 0
     s.variant = {"leaf_flat": 1, "lane_budget": 512, "occupancy": 16, "split": 8, "leaf_handoff": 16}
     assert s.variant == {"leaf_flat": 1, "lane_budget": 512, "occupancy": 16, "split": 8, "leaf_handoff": 16,
-                         "mid_handoff": 0}
+                         "mid_handoff": 0, "edge_triangles": 0}
     s.variant = {"lane_budget": 0}  # 0 keeps the budget
     assert s.variant["lane_budget"] == 512
     with pytest.raises(gi.GIError):
