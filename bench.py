@@ -92,6 +92,9 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-vs-model block")
     ap.add_argument("--no-tune", action="store_true", help="default kernel variants instead of autotuned ones")
+    ap.add_argument("--workload", choices=["six", "clique", "fsm"], default="six",
+                    help="six: the headline six-pattern line; clique / fsm: the Chung-Lu k-clique and labeled FSM "
+                         "workloads, timed and checked against tests/golden/configs.json")
     ap.add_argument("--learned-graphs", type=int, default=16)
     ap.add_argument("--learned-patterns", type=int, default=48)
     return ap.parse_args()
@@ -543,6 +546,81 @@ def run_learned_vs_model(args):
                     "reported as first_pass_s) and one batched launch"}
 
 
+def _configs() -> dict:
+    return json.loads((ROOT / "tests" / "golden" / "configs.json").read_text())
+
+
+def _timed(fn, reps, warm=True):
+    """(result, median seconds) of fn over reps runs (after one warm-up run)."""
+    import torch
+    if warm:
+        fn()
+    ts, out = [], None
+    for _ in range(reps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        out = fn()
+        torch.cuda.synchronize()
+        ts.append(time.perf_counter() - t0)
+    return out, statistics.median(ts)
+
+
+def run_clique(args):
+    """k-cliques on the Chung-Lu graph (3.07M vertices, 117M sampled edges,
+    exponent 2.2): the enumerating bitmap kernel for k = 3..5 and clique-tree
+    pivoting for every k <= 7 in one launch; counts checked against the
+    reference's clique_test (k = 3, 4) and the oracle's pivoting counter
+    (k = 5, 6) recorded in tests/golden/configs.json."""
+    import graphindor_b200 as gi
+    from graphindor_b200 import gen
+    c = _configs()["c3_cliques"]
+    g = gen.chung_lu(**c["params"])
+    t0 = time.perf_counter()
+    dg = gi.Graph.from_csr(g.vertex, g.edge)
+    upload_s = time.perf_counter() - t0
+    want = {int(k): v for k, v in c["cliques"].items()}
+    line = {"metric": "k-clique counting, Chung-Lu 3.07M vertices", "unit": "s", "higher_is_better": False,
+            "data": "synthetic (seeded Chung-Lu)", "upload_s": upload_s, "enumerate": {}, "pivot": {}}
+    for k in (3, 4, 5):
+        r, s = _timed(lambda: gi.clique_count(dg, k, 1), max(1, min(args.steps, 3)))
+        assert r.count == want[k], (k, r.count)
+        line["enumerate"][str(k)] = {"count": r.count, "s": s, "kernel_ms": r.kernel_ms}
+    # The bitmaps the pivoting search runs on were built by the counts above.
+    (counts, st), s = _timed(lambda: gi.clique_counts_pivot(dg, 7, with_stats=True), 1, warm=False)
+    for k, v in want.items():
+        assert counts[k] == v, (k, counts[k])
+    line["pivot"] = {"kmax": 7, "counts": counts, "s": s, "kernel_ms": st.kernel_ms,
+                     "checked": sorted(want)}
+    return line
+
+
+def run_fsm(args):
+    """Labeled FSM on the 100,000-vertex, 29-label R-MAT graph: max_edge 3 at
+    min_support 1000 and 3000, checked against the reference's fsm_test
+    (tests/golden/configs.json); the labeled structure built on the host and
+    on the GPU."""
+    import graphindor_b200 as gi
+    from graphindor_b200 import gen
+    c = _configs()["c3_fsm"]
+    g, labels = gen.labeled_rmat(**c["params"])
+    t0 = time.perf_counter()
+    host = gi.LabeledGraph.from_csr(g.vertex, g.edge, labels)
+    host_s = time.perf_counter() - t0
+    _, dev_s = _timed(lambda: gi.LabeledGraph.from_csr(g.vertex, g.edge, labels, device=True), 3)
+    dev = gi.LabeledGraph.from_csr(g.vertex, g.edge, labels, device=True)
+    line = {"metric": "labeled FSM, R-MAT 100k vertices, 29 labels", "unit": "s", "higher_is_better": False,
+            "data": "synthetic (seeded labeled R-MAT)", "ingest_host_s": host_s, "ingest_device_s": dev_s,
+            "runs": []}
+    for r in c["runs"]:
+        res, s = _timed(lambda: gi.fsm(dev, r["max_edge"], r["min_support"], tri_cnt=7515023),
+                        max(1, min(args.steps, 5)))
+        assert res.count == r["fsm_cnt"], (r, res.count)
+        assert gi.fsm(host, r["max_edge"], r["min_support"], tri_cnt=7515023).count == r["fsm_cnt"]
+        line["runs"].append({"max_edge": r["max_edge"], "min_support": r["min_support"], "fsm_cnt": res.count,
+                             "s": s, "kernel_ms": res.kernel_ms, "reference_fsm_test_s": r["cpu_s"]})
+    return line
+
+
 def main():
     args = parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -551,6 +629,10 @@ def main():
     if args.impl == "reference":
         if rank == 0:
             print(json.dumps(run_reference(args, world)), flush=True)
+        return
+    if args.workload != "six":
+        if rank == 0:
+            print(json.dumps(run_clique(args) if args.workload == "clique" else run_fsm(args)), flush=True)
         return
     if world > 1:
         import datetime

@@ -329,14 +329,16 @@ def clique_count(graph: Graph, k: int, orientation: int = 0, *, count_bytes: boo
     return _result(out.value, s)
 
 
-def clique_counts_pivot(graph: Graph, kmax: int, *, stream: int = 0) -> list[int]:
+def clique_counts_pivot(graph: Graph, kmax: int, *, stream: int = 0, with_stats: bool = False):
     """k-clique counts for every k in [1, kmax] (index k; index 0 is 0) at
-    once, by clique-tree pivoting on the degree-oriented DAG's bitmaps."""
+    once, by clique-tree pivoting on the degree-oriented DAG's bitmaps.  With
+    with_stats, (counts, gi_stats)."""
     out = (C.c_uint64 * (kmax + 1))()
     s = N.Stats()
     check(lib().gi_clique_counts_pivot(graph.handle, kmax, C.c_void_p(stream) if stream else None, out,
                                        C.byref(s)), "gi_clique_counts_pivot")
-    return [int(x) for x in out]
+    counts = [int(x) for x in out]
+    return (counts, s) if with_stats else counts
 
 
 def motif_patterns(k: int) -> list[str]:
