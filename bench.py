@@ -92,9 +92,10 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-vs-model block")
     ap.add_argument("--no-tune", action="store_true", help="default kernel variants instead of autotuned ones")
-    ap.add_argument("--workload", choices=["six", "clique", "fsm"], default="six",
+    ap.add_argument("--workload", choices=["six", "clique", "fsm", "batch"], default="six",
                     help="six: the headline six-pattern line; clique / fsm: the Chung-Lu k-clique and labeled FSM "
-                         "workloads, timed and checked against tests/golden/configs.json")
+                         "workloads, timed and checked against tests/golden/configs.json; batch: the learned-vs-"
+                         "model comparison alone (--learned-graphs, --learned-patterns)")
     ap.add_argument("--learned-graphs", type=int, default=16)
     ap.add_argument("--learned-patterns", type=int, default=48)
     return ap.parse_args()
@@ -632,7 +633,8 @@ def main():
         return
     if args.workload != "six":
         if rank == 0:
-            print(json.dumps(run_clique(args) if args.workload == "clique" else run_fsm(args)), flush=True)
+            run = {"clique": run_clique, "fsm": run_fsm, "batch": run_learned_vs_model}[args.workload]
+            print(json.dumps(run(args)), flush=True)
         return
     if world > 1:
         import datetime
