@@ -592,7 +592,14 @@ def run_clique(args):
         assert counts[k] == v, (k, counts[k])
     line["pivot"] = {"kmax": 7, "counts": counts, "s": s, "kernel_ms": st.kernel_ms,
                      "checked": sorted(want)}
-    return line
+    # All connected 4-vertex motifs (gpu_mc) follow as a line of their own:
+    # the first, the 4-clique, must equal the clique counts above.
+    print(json.dumps(line), flush=True)
+    (motifs, res), s = _timed(lambda: gi.motif_counting(dg, 4), 1, warm=False)
+    assert motifs[0] == want[4], (motifs[0], want[4])
+    return {"metric": "4-vertex motif counting, Chung-Lu 3.07M vertices", "unit": "s", "higher_is_better": False,
+            "counts": motifs, "s": s, "kernel_ms": res.kernel_ms,
+            "checked": "the 4-clique entry equals the clique counts"}
 
 
 def run_fsm(args):
