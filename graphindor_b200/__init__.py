@@ -189,11 +189,11 @@ class Schedule_IEP:
 
 
 def autotune(graph: "Graph", schedule: Schedule_IEP, *, sample_edges: int = 0, max_ms: float = 0.0, reps: int = 0,
-             use_cache: bool = True, stream: int = 0) -> dict:
+             use_cache: bool = True, quick: bool = False, stream: int = 0) -> dict:
     """Times the kernel variants of `schedule` on a sample of `graph` and
     keeps the fastest in the plan (gi_autotune); the choice is cached for the
     class of (plan, graph), and batches apply cached choices to their jobs."""
-    o = N.TuneOptions(int(sample_edges), float(max_ms), int(reps), int(use_cache))
+    o = N.TuneOptions(int(sample_edges), float(max_ms), int(reps), int(use_cache), int(quick))
     info = N.TuneInfo()
     check(lib().gi_autotune(graph.handle, schedule.handle, C.c_void_p(stream) if stream else None, C.byref(o),
                             C.byref(info)), "gi_autotune")
@@ -352,11 +352,11 @@ def motif_patterns(k: int) -> list[str]:
     return [raw[i * k * k:(i + 1) * k * k].decode() for i in range(m)]
 
 
-def motif_counting(graph: Graph, k: int, *, stream: int = 0) -> tuple[list[int], CountResult]:
+def motif_counting(graph: Graph, k: int, *, stream: int = 0, budget_ms: float = 0.0) -> tuple[list[int], CountResult]:
     L = lib()
     m = L.gi_motif_num(k)
     out = (C.c_uint64 * max(1, m))()
-    s = _stats(False)
+    s = _stats(False, budget_ms)
     check(L.gi_motif_count(graph.handle, k, C.c_void_p(stream) if stream else None, out, m, C.byref(s)),
           "gi_motif_count")
     return [int(x) for x in out[:m]], _result(0, s)

@@ -46,8 +46,8 @@ int log2_bucket(int64_t x) {
 }
 
 TuneKey key_of(const gi_graph *g, const DevPlan &P) {
-    return TuneKey{P.n, P.iep_k, P.loop2_kind >= 0 ? 1 : 0, P.first_restricted, log2_bucket(g->e_cnt),
-                   log2_bucket(g->max_degree)};
+    return TuneKey{P.n, P.iep_k, P.loop2_kind >= 0 ? 1 : 0, P.first_restricted, log2_bucket(g->e_cnt) / 2,
+                   log2_bucket(g->max_degree) / 2};
 }
 
 }  // namespace
@@ -120,6 +120,8 @@ int gi_autotune(const gi_graph *g, gi_plan *p, gi_stream stream, const gi_tune_o
         if (opt->max_ms > 0) o.max_ms = opt->max_ms;
         if (opt->reps > 0) o.reps = opt->reps;
         o.use_cache = opt->use_cache;
+        o.quick = opt->quick;
+        if (o.quick) o.reps = 1;
     }
     gi_tune_info res{};
     const TuneKey key = key_of(g, p->dev);
@@ -186,13 +188,19 @@ int gi_autotune(const gi_graph *g, gi_plan *p, gi_stream stream, const gi_tune_o
     int st = GI_OK;
     // Stage 1: the leaf level and the occupancy.
     const int budgets[2] = {256, 2048};
+    const int default_occ = original.occupancy ? original.occupancy : (original.n >= 6 ? 16 : 1);
     std::vector<gi_variant> cands;
-    for (int occ : {1, 16}) {
-        cands.push_back(gi_variant{1, original.lane_budget, occ, 0, 0, 0, 0});
-        for (int b : budgets) cands.push_back(gi_variant{0, b, occ, 0, 0, 0, 0});
+    if (o.quick) {
+        cands.push_back(gi_variant{0, original.lane_budget, default_occ, 0, 0, 0, 0});
+        cands.push_back(gi_variant{1, original.lane_budget, default_occ, 0, 0, 0, 0});
+        cands.push_back(gi_variant{1, original.lane_budget, default_occ == 1 ? 16 : 1, 0, 0, 0, 0});
+    } else {
+        for (int occ : {1, 16}) {
+            cands.push_back(gi_variant{1, original.lane_budget, occ, 0, 0, 0, 0});
+            for (int b : budgets) cands.push_back(gi_variant{0, b, occ, 0, 0, 0, 0});
+        }
     }
     if (original.tri_ok) cands.push_back(gi_variant{0, original.lane_budget, 0, 0, 0, 0, 1});
-    const int default_occ = original.occupancy ? original.occupancy : (original.n >= 6 ? 16 : 1);
     for (const gi_variant &v : cands) {
         double t;
         if ((st = time_variant(v, t)) != GI_OK) break;
@@ -218,7 +226,7 @@ int gi_autotune(const gi_graph *g, gi_plan *p, gi_stream stream, const gi_tune_o
             }
         }
     }
-    if (st == GI_OK && original.leaf_depth >= 2) {
+    if (st == GI_OK && original.leaf_depth >= 2 && !o.quick) {
         for (int lh : {16, 256}) {
             gi_variant v = chosen;
             v.leaf_handoff = lh;

@@ -263,6 +263,9 @@ typedef struct gi_tune_options {
     double max_ms;        /* a variant slower than this on the sample is dropped (0 = 250) */
     int32_t reps;         /* timed runs per variant, the fastest kept (0 = 2) */
     int32_t use_cache;    /* 1: reuse a choice cached for the same class of plan and graph */
+    int32_t quick;        /* 1: a short search (the leaf modes and the edge-triangle path at the
+                             default occupancy, the other occupancy, the split; one run each),
+                             for callers that tune many classes at once */
 } gi_tune_options;
 
 typedef struct gi_tune_info {
@@ -280,7 +283,7 @@ typedef struct gi_tune_info {
  * subset is first resized until the plan's own variant takes between a
  * fiftieth of max_ms and max_ms, starting from sample_edges edges), sets
  * the fastest in p and caches it for the class of (p, g): pattern size, IEP
- * depth, depth-2 split, first-level restriction, log2 of the edge count and
+ * depth, depth-2 split, first-level restriction, log4 of the edge count and
  * of the largest degree.  gi_batch_create applies cached choices to its
  * jobs.  opt and info may be NULL. */
 int gi_autotune(const gi_graph *g, gi_plan *p, gi_stream stream, const gi_tune_options *opt, gi_tune_info *info);
