@@ -64,8 +64,15 @@ def test_missing_model_file_is_an_error(native):
 
 def test_shipped_model_against_the_analytic_choice_on_held_out_patterns():
     """What the trained network gains over the analytic model on the patterns
-    it was not trained on (the committed B200 timings, seeded split): its
-    picks must not be slower in total than the analytic model's."""
+    it was not trained on (the committed B200 timings, seeded 70/30 split by
+    pattern), recomputed from the committed timings and weights: it must
+    equal the figures recorded in report.json, and the learned picks must
+    take less time in total than the analytic model's picks.  The recorded
+    figures: 22 held-out (pattern, graph) cases; learned picks 1,024.5 ms in
+    total against 1,032.3 ms for the analytic picks (0.8 % less; the fastest
+    measured candidate of each case, 983.3 ms); median regret 1.3 % against
+    2.8 %, mean regret 6.4 % against 6.2 %."""
+    import json
     from pathlib import Path
     from graphindor_b200.schedule_cost import train
     here = Path(gi.__file__).resolve().parent / "schedule_cost"
@@ -75,9 +82,11 @@ def test_shipped_model_against_the_analytic_choice_on_held_out_patterns():
     test_p = train.split(keys, 0)
     rep = train.selection_report(keys, 10.0 ** y, pred, [r["model_cost"] for r in runs["rows"]],
                                  {k for k in keys if k[1] in test_p})
+    recorded = json.loads((here / "report.json").read_text())["test"]
+    for k, v in recorded.items():
+        assert rep[k] == pytest.approx(v, rel=1e-5), k
     assert rep["cases"] >= 20
-    assert rep["learned_total_ms"] <= rep["analytic_total_ms"]
-    assert rep["learned_regret_median"] <= rep["analytic_regret_median"]
+    assert rep["learned_total_ms"] < rep["analytic_total_ms"]
 
 
 def test_host_gradient_oracle_matches_finite_differences():
