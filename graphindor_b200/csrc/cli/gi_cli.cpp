@@ -67,6 +67,18 @@ double count_one(gi_graph *g, int n, const char *adj, int iep, bool &ok) {
         report(st, "pattern is invalid!");
         return 0;
     }
+    // The kernel variant for this class of (plan, graph), timed on a sample
+    // before the count (like planning, outside the counting time);
+    // GI_TUNE=0 keeps the default variant.
+    const char *tune = std::getenv("GI_TUNE");
+    if (!tune || std::atoi(tune) != 0) {
+        const double tt = now_s();
+        gi_tune_info ti;
+        if (gi_autotune(g, p, nullptr, nullptr, &ti) == GI_OK)
+            std::fprintf(stderr, "Tuning time: %g seconds (leaf_flat %d, occupancy %d, split %d, edge_triangles %d)\n",
+                         now_s() - tt, ti.chosen.leaf_flat, ti.chosen.occupancy, ti.chosen.split,
+                         ti.chosen.edge_triangles);
+    }
     const double t0 = now_s();
     uint64_t count = 0;
     st = gi_count(g, p, nullptr, &count, nullptr);
