@@ -465,6 +465,9 @@ def random_jobs(n_graphs, n_patterns):
 # its best plan at most this cost (a deterministic filter that keeps each run
 # bounded: sparse 7-vertex patterns on the larger graphs run for hours).
 LEARNED_COST_CAP = 1e7
+# Wall-clock budget of the kernel-variant tuning in the learned arm's first
+# pass (classes not reached keep the default variant).
+LEARNED_TUNE_S = 60.0
 
 
 def run_learned_vs_model(args):
@@ -498,14 +501,19 @@ def run_learned_vs_model(args):
             per.append((time.perf_counter() - j0) * 1e3)
         return time.perf_counter() - t0, counts, per
 
-    def learned_arm():
+    def learned_arm(tune_until=None):
         t0 = time.perf_counter()
         plans = [gi.Schedule_IEP.learned(gi.Pattern(*pats[pi]), graphs[gi_]) for gi_, pi in jobs]
         # Kernel variants: tuned once per class of (plan, graph) on the first
-        # pass, then taken from the tuner's cache.
-        tuned = sum(not gi.autotune(graphs[gi_], p, sample_edges=4096, max_ms=20.0, quick=True)["cached"]
-                    for (gi_, _), p in zip(jobs, plans))
-        tune_counts.append(tuned)
+        # pass while its tuning budget lasts, then taken from the tuner's
+        # cache (classes never tuned keep the default variant).
+        tuned = 0
+        for (gi_, _), p in zip(jobs, plans):
+            live = tune_until is not None and time.perf_counter() < tune_until
+            r = gi.autotune(graphs[gi_], p, sample_edges=4096, max_ms=10.0, quick=True, lookup_only=not live)
+            tuned += live and not r["cached"]
+        if tune_until is not None:
+            tune_counts.append(tuned)
         b = gi.Batch([(graphs[gi_], p) for (gi_, _), p in zip(jobs, plans)])
         counts, lat, kms = b.run()
         return time.perf_counter() - t0, counts, lat, kms, b
@@ -518,10 +526,10 @@ def run_learned_vs_model(args):
     model_arm()
     first_model_s = time.perf_counter() - t_first
     t_first = time.perf_counter()
-    learned_arm()
+    learned_arm(tune_until=t_first + LEARNED_TUNE_S)
     first_learned_s = time.perf_counter() - t_first
     tm, tl, lat, kms = [], [], None, None
-    for r in range(max(1, min(3, args.steps))):
+    for r in range(max(1, min(2, args.steps))):
         for arm in ((0, 1) if r % 2 == 0 else (1, 0)):
             if arm == 0:
                 t, mc, per = model_arm()

@@ -189,11 +189,11 @@ class Schedule_IEP:
 
 
 def autotune(graph: "Graph", schedule: Schedule_IEP, *, sample_edges: int = 0, max_ms: float = 0.0, reps: int = 0,
-             use_cache: bool = True, quick: bool = False, stream: int = 0) -> dict:
+             use_cache: bool = True, quick: bool = False, lookup_only: bool = False, stream: int = 0) -> dict:
     """Times the kernel variants of `schedule` on a sample of `graph` and
     keeps the fastest in the plan (gi_autotune); the choice is cached for the
     class of (plan, graph), and batches apply cached choices to their jobs."""
-    o = N.TuneOptions(int(sample_edges), float(max_ms), int(reps), int(use_cache), int(quick))
+    o = N.TuneOptions(int(sample_edges), float(max_ms), int(reps), int(use_cache), int(quick), int(lookup_only))
     info = N.TuneInfo()
     check(lib().gi_autotune(graph.handle, schedule.handle, C.c_void_p(stream) if stream else None, C.byref(o),
                             C.byref(info)), "gi_autotune")

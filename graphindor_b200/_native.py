@@ -85,7 +85,7 @@ class Variant(C.Structure):
 
 class TuneOptions(C.Structure):
     _fields_ = [("sample_edges", C.c_int64), ("max_ms", C.c_double), ("reps", C.c_int32), ("use_cache", C.c_int32),
-                ("quick", C.c_int32)]
+                ("quick", C.c_int32), ("lookup_only", C.c_int32)]
 
 
 class TuneInfo(C.Structure):

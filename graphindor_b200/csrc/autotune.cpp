@@ -121,6 +121,7 @@ int gi_autotune(const gi_graph *g, gi_plan *p, gi_stream stream, const gi_tune_o
         if (opt->reps > 0) o.reps = opt->reps;
         o.use_cache = opt->use_cache;
         o.quick = opt->quick;
+        o.lookup_only = opt->lookup_only;
         if (o.quick) o.reps = 1;
     }
     gi_tune_info res{};
@@ -136,11 +137,16 @@ int gi_autotune(const gi_graph *g, gi_plan *p, gi_stream stream, const gi_tune_o
             return GI_OK;
         }
     }
+    if (o.lookup_only) {  // nothing cached: the plan keeps its variant
+        res.chosen = variant_of(p->dev);
+        if (info) *info = res;
+        return GI_OK;
+    }
     const DevPlan original = p->dev;
     // Calibrate the sample with the plan's own variant: fewer edges while it
     // runs past max_ms, more while it takes under a fiftieth of it.
     int64_t step = std::max<int64_t>(1, g->e_cnt / std::max<int64_t>(1, o.sample_edges));
-    for (int round = 0; round < 12; ++round) {
+    for (int round = 0; round < (o.quick ? 4 : 12); ++round) {
         gi_stats s{};
         s.edge_step = step;
         s.budget_ms = o.max_ms;

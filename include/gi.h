@@ -266,6 +266,7 @@ typedef struct gi_tune_options {
     int32_t quick;        /* 1: a short search (the leaf modes and the edge-triangle path at the
                              default occupancy, the other occupancy, the split; one run each),
                              for callers that tune many classes at once */
+    int32_t lookup_only;  /* 1: only apply a cached choice; time nothing (cached = 0 when none) */
 } gi_tune_options;
 
 typedef struct gi_tune_info {
