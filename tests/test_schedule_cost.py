@@ -68,10 +68,11 @@ def test_shipped_model_against_the_analytic_choice_on_held_out_patterns():
     pattern), recomputed from the committed timings and weights: it must
     equal the figures recorded in report.json, and the learned picks must
     take less time in total than the analytic model's picks.  The recorded
-    figures: 22 held-out (pattern, graph) cases; learned picks 1,024.5 ms in
-    total against 1,032.3 ms for the analytic picks (0.8 % less; the fastest
-    measured candidate of each case, 983.3 ms); median regret 1.3 % against
-    2.8 %, mean regret 6.4 % against 6.2 %."""
+    figures (weights trained on the B200 by the engine's own kernels,
+    gi_mlp_train): 22 held-out (pattern, graph) cases; learned picks 1,024.1 ms
+    in total against 1,032.3 ms for the analytic picks (0.8 % less; the
+    fastest measured candidate of each case, 983.3 ms); median regret 1.3 %
+    against 2.8 %, mean regret 6.4 % against 6.2 %."""
     import json
     from pathlib import Path
     from graphindor_b200.schedule_cost import train
