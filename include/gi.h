@@ -71,7 +71,8 @@ typedef struct gi_graph_info {
     int32_t max_intersection_size; /* second-largest degree (reference src/dataloader.cpp:297-301) */
     int32_t n_hubs;                /* vertices whose adjacency the counting kernels test through a
                                       bitmap: all of degree >= hub_min_degree (their bitmaps are
-                                      held to 64 MiB per graph by default; GI_HUB_BITMAP_MB) */
+                                      held to 4 GiB per graph by default, at most a sixteenth of the
+                                      free device memory; GI_HUB_BITMAP_MB) */
     int32_t hub_min_degree;
     int32_t hash_min_degree;       /* vertices of at least this degree have an adjacency hash set
                                       (at most 4 GiB per graph by default; GI_HASH_MB) */
