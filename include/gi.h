@@ -287,7 +287,8 @@ typedef struct gi_tune_info {
  * the fastest in p and caches it for the class of (p, g): pattern size, IEP
  * depth, depth-2 split, first-level restriction, log4 of the edge count and
  * of the largest degree.  gi_batch_create applies cached choices to its
- * jobs.  opt and info may be NULL. */
+ * jobs.  opt and info may be NULL.  The call changes p's variant (never its
+ * counts): do not run it while another thread counts with p. */
 int gi_autotune(const gi_graph *g, gi_plan *p, gi_stream stream, const gi_tune_options *opt, gi_tune_info *info);
 int gi_autotune_clear(void);
 
