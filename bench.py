@@ -90,16 +90,14 @@ def parse_args():
     ap.add_argument("--step-scale", type=float, default=1.0,
                     help="divides every edge step (a larger sample); 1 = the pinned subsets")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--learned", action="store_true",
-                    help="add the learned-vs-model block (batched serving shape) to the headline line")
-    ap.add_argument("--no-learned", action="store_true", help="(default) no learned-vs-model block")
+    ap.add_argument("--no-learned", action="store_true", help="skip the learned-vs-model block")
     ap.add_argument("--no-tune", action="store_true", help="default kernel variants instead of autotuned ones")
     ap.add_argument("--workload", choices=["six", "clique", "fsm", "batch"], default="six",
                     help="six: the headline six-pattern line; clique / fsm: the Chung-Lu k-clique and labeled FSM "
                          "workloads, timed and checked against tests/golden/configs.json; batch: the learned-vs-"
                          "model comparison alone (--learned-graphs, --learned-patterns)")
-    ap.add_argument("--learned-graphs", type=int, default=16)
-    ap.add_argument("--learned-patterns", type=int, default=48)
+    ap.add_argument("--learned-graphs", type=int, default=8)
+    ap.add_argument("--learned-patterns", type=int, default=24)
     return ap.parse_args()
 
 
@@ -684,7 +682,7 @@ def main():
         torch.cuda.set_device(local)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=900))
     line, g, tri, raws, divisors = run_ours(args, world, rank, local)
-    if rank == 0 and world == 1 and args.learned and not args.no_learned:
+    if rank == 0 and world == 1 and not args.no_learned:
         line["learned_vs_model"] = run_learned_vs_model(args)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(g, tri, edge_steps(args), os.cpu_count() or 1)
