@@ -220,18 +220,31 @@ __global__ void __launch_bounds__(kBlockThreads, kMinBlocks)
 
 }  // namespace
 
-// Ensures the graph's scratch can hold `bytes`; caller holds g->mu.
+// Ensures the graph's scratch can hold `bytes`; caller holds g->mu.  A
+// growing scratch at least doubles (when the device has the room), so that
+// the plans of a workload, each needing a few more sets than the last, cost
+// few reallocations: each is a device-wide cudaFree and a cudaMalloc of up to
+// gigabytes.
 int ensure_scratch(gi_graph *g, size_t bytes) {
     if (g->scratch_bytes >= bytes) return GI_OK;
     cudaFree(g->d_scratch);
     g->d_scratch = nullptr;
+    const size_t doubled = std::max(bytes, 2 * g->scratch_bytes);
     g->scratch_bytes = 0;
-    cudaError_t e = cudaMalloc(&g->d_scratch, bytes);
+    cudaError_t e = doubled > bytes ? cudaMalloc(&g->d_scratch, doubled) : cudaErrorMemoryAllocation;
+    size_t got = doubled;
     if (e != cudaSuccess) {
         cudaGetLastError();
+        g->d_scratch = nullptr;
+        e = cudaMalloc(&g->d_scratch, bytes);
+        got = bytes;
+    }
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        g->d_scratch = nullptr;
         return cuda_fail(e, "scratch allocation");
     }
-    g->scratch_bytes = bytes;
+    g->scratch_bytes = got;
     return GI_OK;
 }
 
