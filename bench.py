@@ -32,11 +32,17 @@ cpu_baseline / --impl reference: the reference's own CPU code on all host
         src/graph.cpp:305-566) counts them.  The reference arm splits the
         sample over its timed steps, so that over the run it counts exactly
         what one step of this arm counts.
-learned_vs_model: BASELINE's comparison of schedule selection, on whole jobs
-        of the batched-serving shape (seeded random 4-7-vertex patterns on
-        seeded R-MAT graphs of scales 12-18): learned schedules counted in one
+learned_vs_model: the comparison of schedule selection on whole jobs of the
+        batched-serving shape (seeded random 4-7-vertex patterns on seeded
+        R-MAT graphs of scales 12-18; 8 graphs x 24 patterns by default):
+        learned schedules with autotuned kernel variants counted in one
         batched launch against the analytic model's schedules counted one
-        launch per job, planning included, counts asserted equal.
+        launch per job, planning included, counts asserted equal.  Jobs above
+        the analytic cost cap, or whose count runs past 500 ms of device time,
+        are left out of both arms (and reported).
+--workload clique / fsm / batch: the k-clique and FSM workloads on the
+        Chung-Lu and labeled R-MAT graphs (checked against
+        tests/golden/configs.json), or the learned-vs-model block alone.
 """
 from __future__ import annotations
 
